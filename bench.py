@@ -1,0 +1,381 @@
+"""Benchmark of the lattice-Boltzmann node step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 256^3 D3Q19 obstacle flow -- seeded random spheres (radii 4-12,
+10% solid, centres >= 16 cells from the x faces), velocity inlet u=(0.05,0,0)
+at x_min, zero-gradient outlet at x_max, periodic y/z, tau = 0.6, f0 = f_eq(1,0).
+A "step" is one lattice update of all 16.8 M cells; the metric is MLUPS
+(cells x steps / s / 1e6, wall cells included, as the kernel updates them).
+
+* ``value``: K steps of ``lbm_rollout`` on device-resident buffers, timed
+  with CUDA events on the launching stream (state 2 x 1.27 GB > L2, so no
+  flush is needed between steps).
+* ``e2e``: the same K steps through the public ``LBMNode.run`` with the state
+  in pinned host memory: host->device copy of f and the wall mask, the
+  rollout, device->host copy of f, density, velocity and pressure, all inside
+  the timed region (bytes reported per lattice step).
+* ``roofline``: 152 algorithmic bytes per cell-update (19 loads + 19 stores of
+  4 B) over the measured HBM copy bandwidth.
+* ``cpu_baseline``: the CPU restatement of the reference step (the oracle) on
+  a bounded sample of the same workload, on this host's cores.
+* ``--impl reference``: the reference's CPU implementation of the path.  JAX
+  (the reference's array runtime) is not installed on this image, so the
+  restatement of the reference step stands in for it, on all host cores.
+
+Multi-GPU (torchrun, one process per GPU): independent replicas of the
+workload, no collective on the data path ("scaling": "weak").
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRID = (256, 256, 256)
+TAU = 0.6
+U_IN = (0.05, 0.0, 0.0)
+BYTES_PER_CELL = 152  # D3Q19 FP32: 19 x 4 B read + 19 x 4 B written
+METRIC = "MLUPS (D3Q19 FP32 lattice updates/s) & HBM roofline fraction"
+WORKLOAD = "256^3 D3Q19 obstacle flow, velocity inlet + zero-gradient outlet, tau 0.6"
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle restatement): bounded samples
+# ---------------------------------------------------------------------------
+
+def _cpu_sample_worker(args):
+    """One process: float32 restatement of the reference step on a slab of the
+    workload (its first ``nx`` x-planes, same boundary conditions)."""
+    nx, steps, seed = args
+    from oracle import lbm_ref as R
+    from maddening_b200.geometry import random_spheres
+    grid = (nx, GRID[1], GRID[2])
+    wall = random_spheres(GRID, seed=seed)[:nx]
+    node = R.OracleLBM(grid, (TAU - 0.5) / 3.0, "D3Q19", wall_mask=wall,
+                       outlet_condition="zero_gradient", mode="f32")
+    st = node.initial_state()
+    st["f"] = st["f"].astype(np.float32)
+    bi = {"inlet_velocity": np.array(U_IN)}
+    st = node.update(st, bi)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st = node.update(st, bi)
+    dt = time.perf_counter() - t0
+    return nx * GRID[1] * GRID[2] * steps, dt
+
+
+def cpu_baseline(procs: int, nx: int, steps: int):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_sample_worker, [(nx, steps, 0)] * procs)
+        wall_s = time.perf_counter() - t0
+    cells = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return cells / busy / 1e6, wall_s
+
+
+def _host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:  # noqa: BLE001
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def _dist_init():
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def _barrier(world):
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def _max_over_ranks(world, value):
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args):
+    import torch
+    from maddening_b200 import LBMNode, _lib
+    from maddening_b200.geometry import random_spheres
+
+    world, rank, local = _dist_init()
+    dev = torch.device("cuda", local)
+    cells = GRID[0] * GRID[1] * GRID[2]
+    wall = random_spheres(GRID, seed=0)
+    node = LBMNode("bench", 1.0, grid_shape=GRID, viscosity=(TAU - 0.5) / 3.0,
+                   wall_mask=wall, outlet_condition="zero_gradient", device=dev)
+    bi = {"inlet_velocity": np.array(U_IN)}
+
+    # device-resident buffers for the kernel-throughput number
+    st = node.initial_state()
+    f_a = st["f"]
+    f_b = torch.empty_like(f_a)
+    plan = node.plan
+    ws = torch.empty(plan.workspace_bytes(), dtype=torch.uint8, device=dev)
+    sargs, keep = node._step_args(st, bi, dev)
+    rho = torch.empty(GRID, device=dev)
+    vel = torch.empty(GRID + (3,), device=dev)
+    prs = torch.empty(GRID, device=dev)
+    mom = _lib.lbm_moments()
+    mom.density, mom.velocity, mom.pressure = rho.data_ptr(), vel.data_ptr(), prs.data_ptr()
+    lib = _lib.lib()
+    stream = torch.cuda.current_stream(dev)
+
+    def rollout(src, dst, n):
+        _lib.check(lib.lbm_rollout(plan.handle, stream.cuda_stream, src.data_ptr(),
+                                   dst.data_ptr(), int(n), C.byref(sargs), C.byref(mom),
+                                   ws.data_ptr(), ws.numel()))
+
+    rollout(f_a, f_b, max(args.warmup, 3))
+    _barrier(world)
+    K = args.steps
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        _barrier(world)
+        e0.record(stream)
+        rollout(f_b, f_a, K)
+        e1.record(stream)
+        _barrier(world)
+    t_dev = e0.elapsed_time(e1) / 1e3
+    t_dev = _max_over_ranks(world, t_dev)
+    mlups = world * cells * K / t_dev / 1e6
+    clocks = clk.summary()
+
+    # e2e: public API, state in pinned host memory
+    f_host = f_a.cpu().pin_memory()
+    wall_host = torch.as_tensor(wall.astype(np.uint8)).pin_memory()
+    outs = {k: torch.empty(s, dtype=torch.float32).pin_memory() for k, s in
+            (("f", GRID + (19,)), ("density", GRID), ("velocity", GRID + (3,)),
+             ("pressure", GRID))}
+    state_host = {"f": f_host, "wall_mask": wall_host}
+
+    def e2e_once(n):
+        dstate = {"f": state_host["f"].to(dev, non_blocking=True),
+                  "wall_mask": state_host["wall_mask"].to(dev, non_blocking=True)}
+        res = node.run(dstate, bi, n)
+        for k in outs:
+            outs[k].copy_(res[k], non_blocking=True)
+
+    e2e_once(3)
+    _barrier(world)
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    e2e_once(K)
+    e3.record(stream)
+    _barrier(world)
+    t_e2e = _max_over_ranks(world, e2.elapsed_time(e3) / 1e3)
+    h2d = f_host.numel() * 4 + wall_host.numel()
+    d2h = sum(v.numel() * 4 for v in outs.values())
+
+    # variants: other storage forms of the same workload (informational)
+    variants = {}
+    if not args.no_variants:
+        for storage in ("f16", "bf16"):
+            vn = LBMNode("v", 1.0, grid_shape=GRID, viscosity=(TAU - 0.5) / 3.0,
+                         wall_mask=wall, outlet_condition="zero_gradient", storage=storage,
+                         device=dev)
+            vs = vn.initial_state()
+            vn.run(vs, bi, 3)
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            nv = min(K, 200)
+            a0.record(stream)
+            vn.run(vs, bi, nv)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            tv = a0.elapsed_time(a1) / 1e3
+            variants[storage] = {"mlups": round(cells * nv / tv / 1e6, 1), "steps": nv,
+                                 "bytes_per_cell": 76}
+            del vn, vs
+
+    if rank == 0:
+        peak, peak_kind = _peaks()
+        achieved = BYTES_PER_CELL * cells * K / (t_dev / world * world) / 1e9 / 1.0
+        achieved = BYTES_PER_CELL * (cells * K) / t_dev / 1e9  # per GPU
+        line = {
+            "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS",
+            "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": round(t_dev / K * 1e3, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded spheres, rng seed 0)",
+            "config": {"workload": WORKLOAD, "grid": list(GRID), "lattice": "D3Q19",
+                       "storage": "f32 offsets", "tau": TAU, "solid_fraction": float(wall.mean()),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "state 2 x 1.27 GB > 126 MB L2; no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_source": peak_kind, "traffic": None,
+                         "bytes_per_cell": BYTES_PER_CELL,
+                         "kernel": "k_step<19,float,4,0> (fused pull-stream-collide)"},
+            "e2e": {"value": round(world * cells * K / t_e2e / 1e6, 1), "unit": "MLUPS",
+                    "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
+                    "note": "LBMNode.run with pinned-host state in/out, per K-step rollout"},
+            "gpu_launches": K + 1,
+            "clocks": clocks,
+            "variants": variants,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            procs = 1
+            v, _ = cpu_baseline(procs, nx=16, steps=8)
+            line["cpu_baseline"] = {"value": round(v, 3), "unit": "MLUPS", "cores": procs,
+                                    "kind": "port",
+                                    "sample": "float32 oracle restatement, 16x256x256 slab of "
+                                              "the workload, 8 steps, 1 process"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = _host_cores()
+    # each step: every process advances a 16x256x256 slab of the workload by
+    # one step; K steps are bounded to a few minutes in total
+    warm = max(1, min(args.warmup, 1))
+    steps = max(1, min(args.steps, 8))
+    cpu_baseline(procs, nx=16, steps=warm)
+    v, wall_s = cpu_baseline(procs, nx=16, steps=steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MLUPS",
+        "n_gpus": world, "steps": steps, "warmup": warm, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded spheres, rng seed 0)",
+        "config": {"workload": WORKLOAD, "grid": list(GRID)},
+        "cpu_baseline": {"value": round(v, 3), "unit": "MLUPS", "cores": procs, "kind": "port",
+                         "sample": f"{procs} processes x 16x256x256 slab x {steps} steps "
+                                   "(float32 restatement of the reference step; JAX absent)"},
+        "e2e": {"value": round(v, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,164 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 (sm_100a) lattice-Boltzmann node step.
+ *
+ * The library replaces the arithmetic of MADDENING's LBMNode
+ * (src/maddening/nodes/lbm.py, class LBMNode at lbm.py:531-1036).  It is the
+ * surface that an XLA FFI handler (jax.ffi), a torch extension or a ctypes
+ * binding calls: POD arguments, device pointers, a CUDA stream, an int status.
+ *
+ * Conventions
+ *  - Every function returns LBM_OK (0) or a negative lbm_status.  The message
+ *    of the last failure on the calling thread is read with lbm_last_error().
+ *  - No entry point allocates device memory.  Buffers are owned by the caller;
+ *    scratch ("workspace") sizes are queried up front.
+ *  - Layouts are the reference's: a grid_shape (n0, n1[, n2]) C-ordered array
+ *    of cells, populations innermost: f is (*grid_shape, Q), velocity and
+ *    force fields are (*grid_shape, D), density/pressure/wall are grid_shape.
+ *  - Direction order is the reference's (d3q19 at lbm.py:92-135, d2q9 at
+ *    lbm.py:144-169).
+ *  - Floating-point buffers are float32, except for plans with storage
+ *    LBM_STORE_F64, whose f/force/moment buffers are all float64.
+ *  - A plan is immutable after creation; it may be used concurrently from
+ *    several threads on different streams.
+ */
+#ifndef LBM_B200_H_
+#define LBM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+typedef struct CUstream_st* lbm_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  LBM_OK = 0,
+  LBM_ERR_INVALID = -1,     /* bad argument (shape, tau <= 0.5, null ...) */
+  LBM_ERR_UNSUPPORTED = -2, /* valid but not implemented for this plan   */
+  LBM_ERR_CUDA = -3,        /* a CUDA runtime call failed                 */
+  LBM_ERR_WORKSPACE = -4,   /* workspace missing or too small             */
+  LBM_ERR_TIMEOUT = -5      /* a bounded device-side wait gave up         */
+} lbm_status;
+
+typedef enum { LBM_D2Q9 = 9, LBM_D3Q19 = 19 } lbm_lattice;
+
+/* How populations are kept on the device between steps.  All forms store
+ * offsets g_q = f_q - w_q (F16/BF16: normalised, g_q / w_q) and do the
+ * collide arithmetic in FP32 (FP64 for LBM_STORE_F64). */
+typedef enum {
+  LBM_STORE_F32 = 0,
+  LBM_STORE_F16 = 1,
+  LBM_STORE_BF16 = 2,
+  LBM_STORE_F64 = 3
+} lbm_storage;
+
+typedef enum { LBM_FORCE_NONE = 0, LBM_FORCE_UNIFORM = 1, LBM_FORCE_FIELD = 2 } lbm_force_mode;
+
+/* Faces in the order of the reference's _FACE_MAP (lbm.py:517-524). */
+typedef enum {
+  LBM_FACE_X_MIN = 0, LBM_FACE_X_MAX = 1,
+  LBM_FACE_Y_MIN = 2, LBM_FACE_Y_MAX = 3,
+  LBM_FACE_Z_MIN = 4, LBM_FACE_Z_MAX = 5
+} lbm_face;
+
+typedef enum {
+  LBM_BC_NONE = 0,
+  LBM_BC_PRESSURE = 1,      /* reference Zou-He pressure face (lbm.py:425-510);
+                               value[0] = prescribed density rho_p = P / cs2 */
+  LBM_BC_VELOCITY = 2,      /* extension: velocity face, value[0..D-1] = u   */
+  LBM_BC_ZERO_GRADIENT = 3  /* extension: unknown populations copied from the
+                               plane one cell inwards (outlet only)          */
+} lbm_bc_kind;
+
+typedef struct {
+  int32_t kind;     /* lbm_bc_kind */
+  int32_t face;     /* lbm_face    */
+  double value[3];
+} lbm_face_bc;
+
+typedef struct {
+  int32_t lattice;  /* lbm_lattice: 19 (D3Q19) or 9 (D2Q9)                */
+  int32_t storage;  /* lbm_storage                                        */
+  int64_t shape[3]; /* grid_shape; shape[2] is ignored for D2Q9           */
+  double tau;       /* BGK relaxation time, tau = 0.5 + viscosity / cs2    */
+} lbm_desc;
+
+/* Per-call inputs of one step (the reference's boundary_inputs). */
+typedef struct {
+  int32_t force_mode;        /* lbm_force_mode                                   */
+  double force[3];           /* uniform body force (D components)                */
+  const void* force_field;   /* device (*grid_shape, D) when LBM_FORCE_FIELD      */
+  const uint8_t* wall;       /* device grid_shape, nonzero = wall; NULL = none    */
+  lbm_face_bc inlet;         /* applied first  (lbm.py:954-960)                  */
+  lbm_face_bc outlet;        /* applied second (lbm.py:962-968)                  */
+  const float* dev_values;   /* optional device float[9] overriding, in order,
+                                inlet.value[0..2], outlet.value[0..2], force[0..2]
+                                (for values that live on the device, e.g. traced
+                                JAX scalars); NULL = use the host values          */
+} lbm_step_args;
+
+#define LBM_MOMENTS_DENSITY_DEVIATION 1u /* write rho - 1 instead of rho */
+
+/* Outputs of the macroscopic fields (lbm.py:970-976); NULL = not written. */
+typedef struct {
+  void* density;   /* grid_shape                   */
+  void* velocity;  /* (*grid_shape, D), 0 in walls */
+  void* pressure;  /* grid_shape, rho * cs2        */
+  uint32_t flags;
+} lbm_moments;
+
+typedef struct lbm_plan lbm_plan;
+
+int lbm_abi_version(void);
+
+/* Copies the last error message of the calling thread (NUL-terminated). */
+int lbm_last_error(char* buf, size_t len);
+
+/* Validates the lattice/shape/tau like LBMNode.__init__ (lbm.py:604-688). */
+int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan);
+int lbm_plan_destroy(lbm_plan* plan);
+
+/* Bytes of one device copy of the populations in the plan's storage form. */
+int lbm_state_bytes(const lbm_plan* plan, size_t* bytes);
+
+/* Scratch bytes that lbm_update / lbm_rollout need (two population copies). */
+int lbm_workspace_bytes(const lbm_plan* plan, size_t* bytes);
+
+/* f = f_eq(rho, u) (lbm.py:180-206), as initial_state does (lbm.py:719-745).
+ * rho: grid_shape or NULL (= 1); u: (*grid_shape, D) or NULL (= 0). */
+int lbm_equilibrium(const lbm_plan* plan, lbm_stream_t stream, const void* rho,
+                    const void* u, void* f_out);
+
+/* One reference step, LBMNode.update (lbm.py:899-986): macroscopic with F/2,
+ * BGK + Guo collide on every cell, periodic stream on every axis, wall-node
+ * swap, inlet then outlet face, output moments (u = 0 in walls). */
+int lbm_update(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+               void* f_out, const lbm_step_args* args, const lbm_moments* out,
+               void* workspace, size_t workspace_bytes);
+
+/* n_steps >= 1 successive reference steps with the same inputs (the loop body
+ * of GraphManager.run_scan, graph_manager.py:2697-2751).  Between steps the
+ * populations stay on the device as offsets in the plan's storage form; the
+ * moments are those of the last step.  f_in may equal f_out. */
+int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+                void* f_out, int64_t n_steps, const lbm_step_args* args,
+                const lbm_moments* out, void* workspace, size_t workspace_bytes);
+
+/* Scratch bytes of lbm_mass_momentum. */
+int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes);
+
+/* FP64 conservation diagnostics of a state f (*grid_shape, Q):
+ * out_dev[0] = sum rho, out_dev[1..D] = sum_x sum_q f e (device double[4]).
+ * Deterministic (fixed two-pass order). */
+int lbm_mass_momentum(const lbm_plan* plan, lbm_stream_t stream, const void* f,
+                      double* out_dev, void* workspace, size_t workspace_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H_ */

@@ -1,0 +1,363 @@
+// C ABI of the lattice-Boltzmann node step: plan validation, argument
+// mapping and kernel dispatch.  Declarations and contracts: include/lbm_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_kernels.cuh"
+
+struct lbm_plan {
+  int Q = 0, D = 0, storage = 0;
+  int64_t shape[3] = {0, 0, 0};  // reference grid_shape
+  lbm::Geo g{};                  // internal geometry (V-dependent nq / nvec)
+  int V = 1;                     // cells per thread on the step path
+  double tau = 0;
+  size_t elem = 4;               // bytes per stored population
+  size_t io = 4;                 // bytes per f / force / moment element
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return LBM_OK;
+}
+
+size_t state_bytes(const lbm_plan* p) {
+  return static_cast<size_t>(p->Q) * static_cast<size_t>(p->g.ncell) * p->elem;
+}
+
+// Maps one face condition of the ABI to the kernel form (internal axes).
+int map_face(const lbm_plan* p, const lbm_face_bc& in, bool is_outlet, lbm::FaceK* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->kind = lbm::kFaceNone;
+  if (in.kind == LBM_BC_NONE) return LBM_OK;
+  if (in.kind < LBM_BC_NONE || in.kind > LBM_BC_ZERO_GRADIENT)
+    return fail(LBM_ERR_INVALID, "unknown face condition kind %d", in.kind);
+  if (in.face < LBM_FACE_X_MIN || in.face > LBM_FACE_Z_MAX)
+    return fail(LBM_ERR_INVALID, "unknown face %d", in.face);
+  const int ref_axis = in.face / 2;
+  if (ref_axis >= p->D)
+    return fail(LBM_ERR_INVALID,
+                "face %d uses axis %d but lattice D%dQ%d only has %d dimensions", in.face,
+                ref_axis, p->D, p->Q, p->D);
+  const int sh = 3 - p->D;
+  out->kind = in.kind;
+  out->ref_axis = ref_axis;
+  out->axis = ref_axis + sh;
+  out->side = in.face % 2;
+  if (in.kind == LBM_BC_PRESSURE) {
+    out->v[0] = in.value[0];
+  } else if (in.kind == LBM_BC_VELOCITY) {
+    for (int d = 0; d < p->D; ++d) out->v[d + sh] = in.value[d];
+  } else if (in.kind == LBM_BC_ZERO_GRADIENT) {
+    if (!is_outlet) return fail(LBM_ERR_INVALID, "zero-gradient is an outlet condition");
+    if (p->shape[ref_axis] < 3)
+      return fail(LBM_ERR_INVALID, "zero-gradient face needs >= 3 cells along axis %d",
+                  ref_axis);
+  }
+  return LBM_OK;
+}
+
+int build_args(const lbm_plan* p, const lbm_step_args* args, const lbm_moments* mom,
+               lbm::StepArgs* a) {
+  std::memset(a, 0, sizeof(*a));
+  a->g = p->g;
+  a->omega = 1.0 / p->tau;
+  a->guo_c = 1.0 - 0.5 / p->tau;
+  if (args == nullptr) return fail(LBM_ERR_INVALID, "args is NULL");
+  a->force_mode = args->force_mode;
+  const int sh = 3 - p->D;
+  if (args->force_mode == LBM_FORCE_UNIFORM) {
+    for (int d = 0; d < p->D; ++d) a->force[d + sh] = args->force[d];
+  } else if (args->force_mode == LBM_FORCE_FIELD) {
+    if (args->force_field == nullptr)
+      return fail(LBM_ERR_INVALID, "force_mode FIELD needs force_field");
+    a->force_field = args->force_field;
+  } else if (args->force_mode != LBM_FORCE_NONE) {
+    return fail(LBM_ERR_INVALID, "unknown force_mode %d", args->force_mode);
+  }
+  a->wall = args->wall;
+  int rc = map_face(p, args->inlet, false, &a->face[0]);
+  if (rc) return rc;
+  rc = map_face(p, args->outlet, true, &a->face[1]);
+  if (rc) return rc;
+  if (a->face[1].kind == lbm::kFaceZeroGrad && a->face[0].kind != lbm::kFaceNone &&
+      a->face[0].axis != a->face[1].axis)
+    return fail(LBM_ERR_UNSUPPORTED,
+                "a zero-gradient outlet needs the inlet on the same axis (or no inlet)");
+  a->dev_values = args->dev_values;
+  if (mom != nullptr) {
+    a->rho = mom->density;
+    a->vel = mom->velocity;
+    a->prs = mom->pressure;
+    a->mflags = mom->flags;
+  }
+  return LBM_OK;
+}
+
+unsigned grid_for(uint64_t n) { return static_cast<unsigned>((n + lbm::kBlock - 1) / lbm::kBlock); }
+
+template <int Q, class S, int V>
+int launch_prepare(const lbm::StepArgs& a, cudaStream_t s) {
+  lbm::k_prepare<Q, S, V><<<grid_for(a.g.nvec), lbm::kBlock, 0, s>>>(a);
+  return cuda_check(cudaGetLastError(), "k_prepare launch");
+}
+
+template <int Q, class S, int V>
+int launch_step(const lbm::StepArgs& a, bool final_aos, cudaStream_t s) {
+  if (final_aos)
+    lbm::k_step<Q, S, V, lbm::kOutAoS><<<grid_for(a.g.nvec), lbm::kBlock, 0, s>>>(a);
+  else
+    lbm::k_step<Q, S, V, lbm::kOutState><<<grid_for(a.g.nvec), lbm::kBlock, 0, s>>>(a);
+  return cuda_check(cudaGetLastError(), "k_step launch");
+}
+
+// Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies.
+template <int Q, class S, int V>
+int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
+              int64_t n, char* ws) {
+  const size_t sb = state_bytes(p);
+  void* A = ws;
+  void* B = ws + sb;
+  a.f_in = f_in;
+  a.pout = A;
+  int rc = launch_prepare<Q, S, V>(a, s);
+  if (rc) return rc;
+  lbm::StepArgs m = a;  // intermediate steps write no moments
+  m.rho = m.vel = m.prs = nullptr;
+  for (int64_t i = 0; i + 1 < n; ++i) {
+    m.pin = A;
+    m.pout = B;
+    rc = launch_step<Q, S, V>(m, false, s);
+    if (rc) return rc;
+    void* t = A;
+    A = B;
+    B = t;
+  }
+  a.pin = A;
+  a.f_out = f_out;
+  return launch_step<Q, S, V>(a, true, s);
+}
+
+template <int Q, class S>
+int dispatch_v(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a, const void* f_in,
+               void* f_out, int64_t n, char* ws) {
+  constexpr int VV = lbm::StoreT<S>::V;
+  if (p->V == VV) return run_steps<Q, S, VV>(p, s, a, f_in, f_out, n, ws);
+  return run_steps<Q, S, 1>(p, s, a, f_in, f_out, n, ws);
+}
+
+template <int Q>
+int dispatch_s(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a, const void* f_in,
+               void* f_out, int64_t n, char* ws) {
+  switch (p->storage) {
+    case LBM_STORE_F32: return dispatch_v<Q, float>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_F16: return dispatch_v<Q, __half>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_BF16: return dispatch_v<Q, __nv_bfloat16>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_F64: return dispatch_v<Q, double>(p, s, a, f_in, f_out, n, ws);
+  }
+  return fail(LBM_ERR_INVALID, "bad storage");
+}
+
+int do_steps(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* f_out, int64_t n,
+             const lbm_step_args* args, const lbm_moments* out, void* workspace,
+             size_t workspace_bytes, int nbuf) {
+  if (p == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
+  if (f_in == nullptr || f_out == nullptr) return fail(LBM_ERR_INVALID, "f_in/f_out is NULL");
+  if (n < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)n);
+  const size_t need = static_cast<size_t>(nbuf) * state_bytes(p);
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", need,
+                workspace_bytes);
+  lbm::StepArgs a;
+  int rc = build_args(p, args, out, &a);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  return p->Q == 19 ? dispatch_s<19>(p, s, a, f_in, f_out, n, ws)
+                    : dispatch_s<9>(p, s, a, f_in, f_out, n, ws);
+}
+
+constexpr int kReduceBlocks = 148 * 4;
+
+}  // namespace
+
+extern "C" {
+
+int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+int lbm_last_error(char* buf, size_t len) {
+  if (buf == nullptr || len == 0) return LBM_ERR_INVALID;
+  std::snprintf(buf, len, "%s", g_last_error.c_str());
+  return LBM_OK;
+}
+
+int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
+  if (desc == nullptr || plan == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  *plan = nullptr;
+  if (desc->lattice != LBM_D3Q19 && desc->lattice != LBM_D2Q9)
+    return fail(LBM_ERR_INVALID, "Unknown lattice Q=%d. Supported: D3Q19 (19), D2Q9 (9).",
+                desc->lattice);
+  if (desc->storage < LBM_STORE_F32 || desc->storage > LBM_STORE_F64)
+    return fail(LBM_ERR_INVALID, "unknown storage %d", desc->storage);
+  if (!(desc->tau > 0.5) || !std::isfinite(desc->tau))
+    return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g). Increase viscosity.", desc->tau);
+  lbm_plan* p = new lbm_plan();
+  p->Q = desc->lattice;
+  p->D = desc->lattice == LBM_D3Q19 ? 3 : 2;
+  p->storage = desc->storage;
+  p->tau = desc->tau;
+  int64_t dims[3];
+  for (int d = 0; d < p->D; ++d) {
+    if (desc->shape[d] < 1 || desc->shape[d] > (1 << 20)) {
+      delete p;
+      return fail(LBM_ERR_INVALID, "grid_shape[%d] = %lld out of range", d,
+                  (long long)desc->shape[d]);
+    }
+    p->shape[d] = desc->shape[d];
+  }
+  if (p->D == 3) {
+    dims[0] = p->shape[0]; dims[1] = p->shape[1]; dims[2] = p->shape[2];
+  } else {
+    dims[0] = 1; dims[1] = p->shape[0]; dims[2] = p->shape[1];
+  }
+  const int64_t ncell = dims[0] * dims[1] * dims[2];
+  if (ncell >= (int64_t(1) << 32) - 1024) {
+    delete p;
+    return fail(LBM_ERR_INVALID, "lattice of %lld cells is too large", (long long)ncell);
+  }
+  int vv = 4;
+  switch (p->storage) {
+    case LBM_STORE_F32: p->elem = 4; p->io = 4; vv = 4; break;
+    case LBM_STORE_F16:
+    case LBM_STORE_BF16: p->elem = 2; p->io = 4; vv = 4; break;
+    case LBM_STORE_F64: p->elem = 8; p->io = 8; vv = 2; break;
+  }
+  p->V = (dims[2] % vv == 0) ? vv : 1;
+  p->g.n0 = static_cast<int>(dims[0]);
+  p->g.n1 = static_cast<int>(dims[1]);
+  p->g.n2 = static_cast<int>(dims[2]);
+  p->g.nq = static_cast<int>(dims[2] / p->V);
+  p->g.nvec = static_cast<uint32_t>(dims[0] * dims[1] * p->g.nq);
+  p->g.ncell = ncell;
+  *plan = p;
+  return LBM_OK;
+}
+
+int lbm_plan_destroy(lbm_plan* plan) {
+  delete plan;
+  return LBM_OK;
+}
+
+int lbm_state_bytes(const lbm_plan* plan, size_t* bytes) {
+  if (plan == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  *bytes = state_bytes(plan);
+  return LBM_OK;
+}
+
+int lbm_workspace_bytes(const lbm_plan* plan, size_t* bytes) {
+  if (plan == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  *bytes = 2 * state_bytes(plan);
+  return LBM_OK;
+}
+
+int lbm_equilibrium(const lbm_plan* p, lbm_stream_t stream, const void* rho, const void* u,
+                    void* f_out) {
+  if (p == nullptr || f_out == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const unsigned grid = grid_for(static_cast<uint64_t>(p->g.ncell));
+  if (p->io == 8) {
+    if (p->Q == 19)
+      lbm::k_equilibrium<19, double><<<grid, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const double*>(rho), static_cast<const double*>(u),
+          static_cast<double*>(f_out));
+    else
+      lbm::k_equilibrium<9, double><<<grid, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const double*>(rho), static_cast<const double*>(u),
+          static_cast<double*>(f_out));
+  } else {
+    if (p->Q == 19)
+      lbm::k_equilibrium<19, float><<<grid, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const float*>(rho), static_cast<const float*>(u),
+          static_cast<float*>(f_out));
+    else
+      lbm::k_equilibrium<9, float><<<grid, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const float*>(rho), static_cast<const float*>(u),
+          static_cast<float*>(f_out));
+  }
+  return cuda_check(cudaGetLastError(), "k_equilibrium launch");
+}
+
+int lbm_update(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, void* f_out,
+               const lbm_step_args* args, const lbm_moments* out, void* workspace,
+               size_t workspace_bytes) {
+  return do_steps(plan, stream, f_in, f_out, 1, args, out, workspace, workspace_bytes, 1);
+}
+
+int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, void* f_out,
+                int64_t n_steps, const lbm_step_args* args, const lbm_moments* out,
+                void* workspace, size_t workspace_bytes) {
+  return do_steps(plan, stream, f_in, f_out, n_steps, args, out, workspace, workspace_bytes,
+                  n_steps > 1 ? 2 : 1);
+}
+
+int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes) {
+  if (plan == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  *bytes = sizeof(double) * 4 * kReduceBlocks;
+  return LBM_OK;
+}
+
+int lbm_mass_momentum(const lbm_plan* p, lbm_stream_t stream, const void* f, double* out_dev,
+                      void* workspace, size_t workspace_bytes) {
+  if (p == nullptr || f == nullptr || out_dev == nullptr)
+    return fail(LBM_ERR_INVALID, "NULL argument");
+  const size_t need = sizeof(double) * 4 * kReduceBlocks;
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", need,
+                workspace_bytes);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  double* part = static_cast<double*>(workspace);
+  const double nc = static_cast<double>(p->g.ncell);
+  if (p->io == 8) {
+    if (p->Q == 19) {
+      lbm::k_mass_momentum_part<19, double><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const double*>(f), part);
+      lbm::k_mass_momentum_final<19><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+    } else {
+      lbm::k_mass_momentum_part<9, double><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const double*>(f), part);
+      lbm::k_mass_momentum_final<9><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+    }
+  } else {
+    if (p->Q == 19) {
+      lbm::k_mass_momentum_part<19, float><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const float*>(f), part);
+      lbm::k_mass_momentum_final<19><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+    } else {
+      lbm::k_mass_momentum_part<9, float><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+          p->g, static_cast<const float*>(f), part);
+      lbm::k_mass_momentum_final<9><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+    }
+  }
+  return cuda_check(cudaGetLastError(), "k_mass_momentum launch");
+}
+
+}  // extern "C"

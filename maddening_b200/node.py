@@ -1,0 +1,404 @@
+"""``LBMNode``: the reference's lattice-Boltzmann node on B200 kernels.
+
+Drop-in for MADDENING's ``LBMNode`` (``src/maddening/nodes/lbm.py:531-1036``):
+same constructor arguments, validation messages, state keys and dtypes,
+boundary inputs and ``update`` semantics.  The arithmetic runs in the sm_100a
+kernels of ``liblbm_b200.so`` through its C ABI; state arrays are torch CUDA
+tensors (the caching allocator owns them).  There is no CPU path: without a
+CUDA device or without the built library the calls raise.
+
+Additions beyond the reference (documented extensions):
+
+* ``run(state, boundary_inputs, n_steps)`` -- ``n_steps`` reference steps in
+  one call, populations kept on the device as offsets between steps.
+* boundary input ``inlet_velocity`` (D,) -- velocity face at ``inlet_face``.
+* ``outlet_condition="zero_gradient"`` -- zero-gradient face at
+  ``outlet_face`` on every step.
+* ``storage`` -- how populations are held between steps inside ``run``:
+  ``"f32"`` (default), ``"f16"``/``"bf16"`` (normalised offsets, FP32
+  arithmetic) or ``"f64"`` (FP64 throughout; state arrays are float64).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from .contract import (BoundaryInputSpec, NodeMeta, SimulationNode, StabilityLevel,
+                       ValidatedRegime)
+from .lattice import by_name
+
+_FACE_MAP = {"x_min": (0, "min"), "x_max": (0, "max"), "y_min": (1, "min"),
+             "y_max": (1, "max"), "z_min": (2, "min"), "z_max": (2, "max")}
+
+
+def prescribed_density(pressure, cs2: float = 1.0 / 3.0):
+    """``pressure / cs2`` the way the reference evaluates it (lbm.py:956).
+
+    cs2 is a weak Python scalar: a float32 input divides in float32, a
+    float64 or Python input in float64.  Returns a Python float for host
+    inputs and a 0-d CUDA tensor for device inputs.
+    """
+    if isinstance(pressure, torch.Tensor):
+        if pressure.is_cuda:
+            return pressure.reshape(()) / cs2
+        pressure = pressure.numpy()
+    p = np.asarray(pressure)
+    if p.dtype == np.float32:
+        return float(np.float32(p) / np.float32(cs2))
+    return float(np.float64(p) / cs2)
+
+
+class LBMNode(SimulationNode):
+    """BGK lattice-Boltzmann node (D3Q19 / D2Q9) with wall-node bounce-back,
+    Zou-He pressure faces and Guo body forcing, on sm_100a kernels."""
+
+    meta = NodeMeta(
+        algorithm_id="MADD-NODE-007",
+        algorithm_version="1.0.0",
+        stability=StabilityLevel.EXPERIMENTAL,
+        description=("General LBM node with BGK collision, Zou-He pressure BCs, "
+                     "and arbitrary wall-mask domains (B200 kernels)"),
+        governing_equations=("BGK collision: f_i = f_i - (f_i - f_eq_i)/tau + S_guo; "
+                             "streaming: f_i(x+e_i, t+1) = f_i(x, t)"),
+        discretization="Lattice Boltzmann (D3Q19/D2Q9, explicit, 2nd-order)",
+        assumptions=("Incompressible flow (Mach number << 1)",
+                     "BGK single-relaxation-time collision operator",
+                     "Rigid, impermeable walls (wall-node bounce-back)",
+                     "Zou-He pressure boundary conditions at inlet/outlet"),
+        limitations=("Compressibility errors at high Mach number (Ma > 0.1)",
+                     "BGK is less stable than MRT for high Reynolds numbers",
+                     "No turbulence model",
+                     "Wall bounce-back is 1st-order at curved boundaries"),
+        validated_regimes=(ValidatedRegime("tau", 0.501, 2.0,
+                                           notes="tau > 0.5 required"),),
+        hazard_hints=("Behaviour uncharacterised at Re > 100",
+                      "Wall bounce-back assumes rigid, impermeable walls"),
+    )
+
+    def __init__(self, name: str, timestep: float, grid_shape: tuple = (64, 32, 32),
+                 viscosity: float = 0.1, lattice: str = "D3Q19",
+                 wall_mask: Optional[np.ndarray] = None, inlet_face: str = "x_min",
+                 outlet_face: str = "x_max", geometry_source: Optional[str] = None,
+                 *, outlet_condition: str = "pressure", storage: str = "f32",
+                 device=None):
+        lat = by_name(lattice)
+        if len(grid_shape) != lat.D:
+            raise ValueError(f"grid_shape has {len(grid_shape)} dims but lattice "
+                             f"{lat.name} requires {lat.D} dims.")
+        tau = 0.5 + viscosity / lat.cs2
+        if tau <= 0.5:
+            raise ValueError(f"tau must be > 0.5 (got {tau}). Increase viscosity.")
+        for face_name, face_label in (("inlet_face", inlet_face), ("outlet_face", outlet_face)):
+            if face_label not in _FACE_MAP:
+                raise ValueError(f"Unknown {face_name} '{face_label}'. "
+                                 f"Supported: {list(_FACE_MAP.keys())}")
+            axis, _ = _FACE_MAP[face_label]
+            if axis >= lat.D:
+                raise ValueError(f"{face_name} '{face_label}' uses axis {axis} but lattice "
+                                 f"{lat.name} only has {lat.D} dimensions.")
+        if outlet_condition not in ("pressure", "zero_gradient"):
+            raise ValueError(f"Unknown outlet_condition '{outlet_condition}'. "
+                             "Supported: ['pressure', 'zero_gradient']")
+        if storage not in _lib.STORAGE:
+            raise ValueError(f"Unknown storage '{storage}'. Supported: {list(_lib.STORAGE)}")
+        super().__init__(name, timestep, grid_shape=grid_shape, viscosity=viscosity,
+                         lattice=lattice, inlet_face=inlet_face, outlet_face=outlet_face,
+                         geometry_source=geometry_source)
+        self._lat = lat
+        self._grid_shape = tuple(int(n) for n in grid_shape)
+        self._D = lat.D
+        self._Q = lat.Q
+        self._tau = tau
+        self._cs2 = lat.cs2
+        self._inlet_face = inlet_face
+        self._outlet_face = outlet_face
+        self._outlet_condition = outlet_condition
+        self._storage = storage
+        self._io_dtype = torch.float64 if storage == "f64" else torch.float32
+        self._device = torch.device(device) if device is not None else None
+        if wall_mask is not None:
+            wall_mask = np.asarray(wall_mask)
+            if wall_mask.shape != self._grid_shape:
+                raise ValueError(f"wall_mask shape {wall_mask.shape} != grid_shape "
+                                 f"{self._grid_shape}")
+            self._wall_np = wall_mask.astype(bool)
+        else:
+            self._wall_np = np.zeros(self._grid_shape, dtype=bool)
+        self._has_walls = bool(self._wall_np.any())
+        self._wall_dev = {}
+        self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage)
+
+    # -- properties (lbm.py:690-703) ---------------------------------------
+    @property
+    def tau(self) -> float:
+        return self._tau
+
+    @property
+    def viscosity(self) -> float:
+        return self._cs2 * (self._tau - 0.5)
+
+    @property
+    def lattice(self):
+        return self._lat
+
+    @property
+    def storage(self) -> str:
+        return self._storage
+
+    @property
+    def plan(self) -> _lib.Plan:
+        return self._plan
+
+    # -- contract ------------------------------------------------------------
+    def halo_width(self) -> dict:
+        """One ghost cell per side on every spatial axis (lbm.py:709-717)."""
+        return {axis: 1 for axis in range(self._D)}
+
+    @property
+    def requires_halo(self) -> bool:
+        """Pre-v0.3 spelling of ``bool(halo_width())``."""
+        return bool(self.halo_width())
+
+    def _dev(self) -> torch.device:
+        if not torch.cuda.is_available():
+            raise RuntimeError("LBMNode needs a CUDA device (sm_100a); there is no CPU path")
+        if self._device is None:
+            self._device = torch.device("cuda", torch.cuda.current_device())
+        return self._device
+
+    def _wall_mask_on(self, dev) -> torch.Tensor:
+        key = str(dev)
+        if key not in self._wall_dev:
+            self._wall_dev[key] = torch.as_tensor(self._wall_np.astype(np.uint8), device=dev)
+        return self._wall_dev[key]
+
+    def initial_state(self) -> dict:
+        """rho = 1, u = 0, f = f_eq, p = rho cs2, wall_mask uint8 (lbm.py:719-745)."""
+        dev = self._dev()
+        shape = self._grid_shape
+        density = torch.ones(shape, dtype=self._io_dtype, device=dev)
+        velocity = torch.zeros(shape + (self._D,), dtype=self._io_dtype, device=dev)
+        f = self.equilibrium(None, None)
+        pressure = density * self._cs2
+        return {"f": f, "density": density, "velocity": velocity, "pressure": pressure,
+                "wall_mask": self._wall_mask_on(dev).clone()}
+
+    def equilibrium(self, density=None, velocity=None) -> torch.Tensor:
+        """f_eq(rho, u) on the device (lbm.py:180-206); None means rho=1 / u=0."""
+        dev = self._dev()
+        f = torch.empty(self._grid_shape + (self._Q,), dtype=self._io_dtype, device=dev)
+        rho = None if density is None else self._as_field(density, self._grid_shape, dev)
+        u = None if velocity is None else self._as_field(velocity, self._grid_shape + (self._D,), dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_equilibrium(
+            self._plan.handle, stream, None if rho is None else rho.data_ptr(),
+            None if u is None else u.data_ptr(), f.data_ptr()))
+        return f
+
+    def _as_field(self, x, shape, dev) -> torch.Tensor:
+        t = torch.as_tensor(x, device=dev).to(self._io_dtype)
+        if tuple(t.shape) != tuple(shape):
+            raise ValueError(f"expected shape {tuple(shape)}, got {tuple(t.shape)}")
+        return t.contiguous()
+
+    # -- boundary inputs (lbm.py:910-968) ------------------------------------
+    def _step_args(self, state: dict, bi: dict, dev):
+        """Builds the C step arguments; returns (args, keep-alive tensors)."""
+        a = _lib.lbm_step_args()
+        keep = []
+        D = self._D
+        # wall mask precedence: wall_mask_update > state["wall_mask"] > node mask
+        if "wall_mask_update" in bi:
+            wall = torch.as_tensor(bi["wall_mask_update"], device=dev)
+        elif "wall_mask" in state:
+            wall = torch.as_tensor(state["wall_mask"], device=dev)
+        else:
+            wall = self._wall_mask_on(dev)
+        if tuple(wall.shape) != self._grid_shape:
+            raise ValueError(f"wall mask shape {tuple(wall.shape)} != grid_shape "
+                             f"{self._grid_shape}")
+        wall = (wall != 0).to(torch.uint8).contiguous() if wall.dtype != torch.uint8 \
+            else wall.contiguous()
+        keep.append(wall)
+        a.wall = wall.data_ptr()
+
+        dev_vals = [None] * 9  # inlet[3], outlet[3], force[3]
+        use_dev = False
+
+        force = bi.get("body_force", None)
+        if force is None:
+            a.force_mode = _lib.FORCE_NONE
+        else:
+            ft = force if isinstance(force, torch.Tensor) else torch.as_tensor(np.asarray(force))
+            if ft.ndim == 1 and tuple(ft.shape) == (D,):
+                a.force_mode = _lib.FORCE_UNIFORM
+                if ft.is_cuda:
+                    use_dev = True
+                    for d in range(D):
+                        dev_vals[6 + d] = ft[d].to(torch.float32)
+                else:
+                    vals = ft.to(torch.float32).numpy()  # the reference casts to float32
+                    for d in range(D):
+                        a.force[d] = float(vals[d])
+                        dev_vals[6 + d] = float(vals[d])
+            else:
+                field = self._as_field(ft, self._grid_shape + (D,), dev)
+                keep.append(field)
+                a.force_mode = _lib.FORCE_FIELD
+                a.force_field = field.data_ptr()
+
+        p_in = bi.get("inlet_pressure", None)
+        u_in = bi.get("inlet_velocity", None)
+        p_out = bi.get("outlet_pressure", None)
+        if p_in is not None and u_in is not None:
+            raise ValueError("inlet_pressure and inlet_velocity are exclusive")
+
+        def set_face(face: _lib.lbm_face_bc, slot: int, kind: int, label: str, value):
+            nonlocal use_dev
+            face.kind = kind
+            face.face = _lib.FACES[label]
+            if kind == _lib.BC_PRESSURE:
+                rho = prescribed_density(value, self._cs2)
+                if isinstance(rho, torch.Tensor):
+                    use_dev = True
+                    dev_vals[slot] = rho.to(torch.float32)
+                else:
+                    face.value[0] = rho
+                    dev_vals[slot] = rho
+            elif kind == _lib.BC_VELOCITY:
+                ut = value if isinstance(value, torch.Tensor) else torch.as_tensor(np.asarray(value))
+                if tuple(ut.shape) != (D,):
+                    raise ValueError(f"inlet_velocity must have shape ({D},)")
+                if ut.is_cuda:
+                    use_dev = True
+                    for d in range(D):
+                        dev_vals[slot + d] = ut[d].to(torch.float32)
+                else:
+                    for d, v in enumerate(ut.to(torch.float64).numpy()):
+                        face.value[d] = float(v)
+                        dev_vals[slot + d] = float(v)
+
+        if p_in is not None:
+            set_face(a.inlet, 0, _lib.BC_PRESSURE, self._inlet_face, p_in)
+        elif u_in is not None:
+            set_face(a.inlet, 0, _lib.BC_VELOCITY, self._inlet_face, u_in)
+        if self._outlet_condition == "zero_gradient":
+            set_face(a.outlet, 3, _lib.BC_ZERO_GRADIENT, self._outlet_face, None)
+        elif p_out is not None:
+            set_face(a.outlet, 3, _lib.BC_PRESSURE, self._outlet_face, p_out)
+
+        if use_dev:
+            parts = [v if isinstance(v, torch.Tensor) else
+                     torch.tensor(0.0 if v is None else v, dtype=torch.float32, device=dev)
+                     for v in dev_vals]
+            dv = torch.stack([p.reshape(()).to(device=dev, dtype=torch.float32) for p in parts])
+            keep.append(dv)
+            a.dev_values = dv.data_ptr()
+        return a, keep
+
+    def _outputs(self, dev):
+        shape = self._grid_shape
+        f = torch.empty(shape + (self._Q,), dtype=self._io_dtype, device=dev)
+        rho = torch.empty(shape, dtype=self._io_dtype, device=dev)
+        vel = torch.empty(shape + (self._D,), dtype=self._io_dtype, device=dev)
+        prs = torch.empty(shape, dtype=self._io_dtype, device=dev)
+        m = _lib.lbm_moments()
+        m.density, m.velocity, m.pressure = rho.data_ptr(), vel.data_ptr(), prs.data_ptr()
+        return f, rho, vel, prs, m
+
+    def _f_in(self, state, dev) -> torch.Tensor:
+        f = state["f"]
+        f = torch.as_tensor(f, device=dev)
+        if f.dtype != self._io_dtype:
+            f = f.to(self._io_dtype)
+        if tuple(f.shape) != self._grid_shape + (self._Q,):
+            raise ValueError(f"state['f'] shape {tuple(f.shape)} != "
+                             f"{self._grid_shape + (self._Q,)}")
+        return f.contiguous()
+
+    def _advance(self, state: dict, boundary_inputs: dict, n_steps: int) -> dict:
+        dev = self._dev()
+        f_in = self._f_in(state, dev)
+        args, keep = self._step_args(state, boundary_inputs or {}, dev)
+        f, rho, vel, prs, m = self._outputs(dev)
+        nbuf = 2 if n_steps > 1 else 1
+        ws = torch.empty(nbuf * self._plan.state_bytes(), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        lib = _lib.lib()
+        if n_steps == 1:
+            rc = lib.lbm_update(self._plan.handle, stream, f_in.data_ptr(), f.data_ptr(),
+                                C.byref(args), C.byref(m), ws.data_ptr(), ws.numel())
+        else:
+            rc = lib.lbm_rollout(self._plan.handle, stream, f_in.data_ptr(), f.data_ptr(),
+                                 int(n_steps), C.byref(args), C.byref(m), ws.data_ptr(),
+                                 ws.numel())
+        _lib.check(rc)
+        del keep
+        out = {"f": f, "density": rho, "velocity": vel, "pressure": prs}
+        if "wall_mask" in state:
+            out["wall_mask"] = state["wall_mask"]
+        return out
+
+    def update(self, state: dict, boundary_inputs: dict, dt: float) -> dict:
+        """One reference step (lbm.py:899-986)."""
+        return self._advance(state, boundary_inputs, 1)
+
+    def run(self, state: dict, boundary_inputs: dict, n_steps: int) -> dict:
+        """``n_steps`` reference steps with the same boundary inputs, fused."""
+        if int(n_steps) < 1:
+            raise ValueError("n_steps must be >= 1")
+        return self._advance(state, boundary_inputs, int(n_steps))
+
+    def update_padded(self, state_padded, boundary_inputs, dt, *, static_padded=None,
+                      shard_info=None):
+        raise NotImplementedError(
+            "LBMNode (B200) runs on one GPU; the halo-padded sharded step "
+            "(update_padded) is not provided")
+
+    def derivatives(self, state: dict, boundary_inputs: dict) -> dict:
+        raise NotImplementedError(
+            "LBMNode uses a discrete lattice Boltzmann update, "
+            "not a continuous ODE. derivatives() is not applicable.")
+
+    def compute_boundary_fluxes(self, state: dict, boundary_inputs: dict, dt: float) -> dict:
+        """Mean pressure over the fluid cells of the outlet face (lbm.py:995-1017)."""
+        pressure = torch.as_tensor(state["pressure"])
+        axis, side = _FACE_MAP[self._outlet_face]
+        idx = [slice(None)] * self._D
+        idx[axis] = 0 if side == "min" else -1
+        idx = tuple(idx)
+        wall = torch.as_tensor(self._wall_np[idx], device=pressure.device)
+        p_face = pressure[idx]
+        fluid = (~wall).sum().to(pressure.dtype)
+        p_sum = torch.where(wall, torch.zeros_like(p_face), p_face).sum()
+        return {"outlet_pressure_avg": p_sum / torch.clamp(fluid, min=1.0)}
+
+    def boundary_input_spec(self) -> dict:
+        return {
+            "inlet_pressure": BoundaryInputSpec(shape=(), description="Zou-He pressure at inlet face"),
+            "outlet_pressure": BoundaryInputSpec(shape=(), description="Zou-He pressure at outlet face"),
+            "inlet_velocity": BoundaryInputSpec(shape=(self._D,),
+                                                description="Velocity at inlet face (extension)"),
+            "body_force": BoundaryInputSpec(shape=(*self._grid_shape, self._D),
+                                            coupling_type="additive",
+                                            description="External body force field"),
+            "wall_mask_update": BoundaryInputSpec(shape=self._grid_shape,
+                                                  description="Runtime wall mask override (True=wall)"),
+        }
+
+    # -- diagnostics -----------------------------------------------------------
+    def mass_momentum(self, f) -> torch.Tensor:
+        """FP64 (sum rho, sum rho u) of a state f, reduced on the device."""
+        dev = self._dev()
+        f = self._f_in({"f": f}, dev)
+        out = torch.empty(4, dtype=torch.float64, device=dev)
+        ws = torch.empty(self._plan.reduce_workspace_bytes(), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_mass_momentum(self._plan.handle, stream, f.data_ptr(),
+                                                out.data_ptr(), ws.data_ptr(), ws.numel()))
+        return out[: 1 + self._D]

@@ -1,0 +1,356 @@
+"""Generate golden vectors by executing the reference's own ``lbm.py``.
+
+JAX is not installed in this container (and has no offline wheel), so the
+reference module ``maddening.nodes.lbm`` cannot be imported as shipped.  This
+script executes that unmodified source file against a small NumPy-backed
+stand-in for the ``jax`` API subset it uses (``jnp.roll/stack/where/sum/...``
+and functional ``x.at[idx].set(v)`` updates).  Two arithmetic modes are
+emulated:
+
+* ``x64``: NumPy float64 constants promote float32 arrays -- the reference
+  under ``jax_enable_x64`` (the FP64 oracle the build is graded against).
+* ``f32``: float64 NumPy constants are demoted to float32 whenever they meet
+  a stand-in array -- JAX's default canonicalisation (informational only:
+  XLA may order float32 roundings differently).
+
+The package ``__init__`` files of ``maddening.core`` and ``maddening.nodes``
+import JAX-heavy siblings; they are bypassed by registering bare package
+modules whose ``__path__`` points at the real directories, so only
+``core/node.py``, ``core/compliance/*`` and ``nodes/lbm.py`` execute.
+
+Run from the repository root (needs the reference checkout)::
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+It rewrites ``tests/golden/lbm_golden.npz``.  The fixtures are committed;
+nothing at test time reads the reference.
+"""
+
+from __future__ import annotations
+
+import importlib
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+MODE = {"value": "x64"}
+
+
+# ---------------------------------------------------------------------------
+# NumPy-backed stand-in for the jax API subset used by nodes/lbm.py
+# ---------------------------------------------------------------------------
+
+
+class JArray(np.ndarray):
+    """ndarray with JAX's functional ``.at[idx].set(v)`` update."""
+
+    @property
+    def at(self):
+        return _At(self)
+
+    def __array_ufunc__(self, ufunc, method, *inputs, **kwargs):
+        conv = []
+        for x in inputs:
+            if isinstance(x, JArray):
+                x = x.view(np.ndarray)
+            elif MODE["value"] == "f32" and isinstance(x, np.ndarray) \
+                    and x.dtype == np.float64:
+                x = x.astype(np.float32)
+            conv.append(x)
+        if "out" in kwargs:
+            kwargs["out"] = tuple(o.view(np.ndarray) if isinstance(o, JArray) else o
+                                  for o in kwargs["out"])
+        res = getattr(ufunc, method)(*conv, **kwargs)
+        return _wrap(res)
+
+
+class _At:
+    def __init__(self, arr):
+        self.arr = arr
+
+    def __getitem__(self, idx):
+        return _AtIdx(self.arr, idx)
+
+
+class _AtIdx:
+    def __init__(self, arr, idx):
+        self.arr, self.idx = arr, idx
+
+    def set(self, value):
+        out = np.array(self.arr, copy=True)
+        out[self.idx] = np.asarray(value)
+        return out.view(JArray)
+
+
+def _wrap(x):
+    if isinstance(x, tuple):
+        return tuple(_wrap(v) for v in x)
+    if isinstance(x, np.ndarray):
+        if MODE["value"] == "f32" and x.dtype == np.float64:
+            x = x.astype(np.float32)
+        return x.view(JArray)
+    return x
+
+
+def _plain(x):
+    return x.view(np.ndarray) if isinstance(x, JArray) else x
+
+
+def _make_jnp():
+    jnp = types.ModuleType("jax.numpy")
+    for name in ("float32", "float64", "int32", "uint8", "bool_"):
+        setattr(jnp, name, getattr(np, name))
+
+    def asarray(x, dtype=None):
+        a = np.asarray(_plain(x), dtype=dtype)
+        return _wrap(np.array(a, copy=True))
+
+    def zeros(shape, dtype=None):
+        return _wrap(np.zeros(shape, dtype=dtype if dtype is not None else np.float32))
+
+    def ones(shape, dtype=None):
+        return _wrap(np.ones(shape, dtype=dtype if dtype is not None else np.float32))
+
+    jnp.asarray = asarray
+    jnp.array = asarray
+    jnp.zeros = zeros
+    jnp.ones = ones
+    jnp.zeros_like = lambda x, dtype=None: _wrap(np.zeros_like(_plain(x), dtype=dtype))
+    jnp.full_like = lambda x, v, dtype=None: _wrap(np.full_like(_plain(x), _plain(v), dtype=dtype))
+    jnp.sum = lambda x, axis=None, keepdims=False: _wrap(np.sum(_plain(x), axis=axis, keepdims=keepdims))
+    jnp.maximum = lambda a, b: _wrap(np.maximum(_plain(a), _plain(b)))
+    jnp.roll = lambda x, s, axis=None: _wrap(np.roll(_plain(x), s, axis=axis))
+    jnp.stack = lambda xs, axis=0: _wrap(np.stack([_plain(v) for v in xs], axis=axis))
+    jnp.where = lambda c, a, b: _wrap(np.where(_plain(c), _plain(a), _plain(b)))
+    jnp.broadcast_to = lambda x, shape: _wrap(np.broadcast_to(_plain(x), shape))
+    jnp.pad = lambda x, w: _wrap(np.pad(_plain(x), w))
+    jnp.all = lambda x: bool(np.all(_plain(x)))
+    jnp.isfinite = lambda x: _wrap(np.isfinite(_plain(x)))
+    jnp.ndarray = JArray
+    return jnp
+
+
+def _install_shims(ref_root: Path):
+    jax = types.ModuleType("jax")
+    jnp = _make_jnp()
+    lax = types.ModuleType("jax.lax")
+
+    def slice_in_dim(x, start, limit, axis=0):
+        sl = [slice(None)] * np.ndim(x)
+        sl[axis] = slice(start, limit)
+        return _wrap(np.asarray(_plain(x))[tuple(sl)])
+
+    lax.slice_in_dim = slice_in_dim
+    jax.numpy = jnp
+    jax.lax = lax
+    sys.modules["jax"] = jax
+    sys.modules["jax.numpy"] = jnp
+    sys.modules["jax.lax"] = lax
+
+    src = ref_root / "src"
+    sys.path.insert(0, str(src))
+    import maddening  # noqa: F401  (lazy __init__, no jax import)
+    for pkg in ("maddening.core", "maddening.nodes"):
+        mod = types.ModuleType(pkg)
+        mod.__path__ = [str(src / Path(*pkg.split(".")))]
+        sys.modules[pkg] = mod
+    return importlib.import_module("maddening.nodes.lbm")
+
+
+# ---------------------------------------------------------------------------
+# Cases
+# ---------------------------------------------------------------------------
+
+
+def _perturbed_f(lbm, node, seed, amp=1e-3):
+    st = node.initial_state()
+    f = np.asarray(_plain(st["f"]), dtype=np.float64)
+    w = node._lat.w
+    rng = np.random.default_rng(seed)
+    f = f + amp * w * rng.standard_normal(f.shape)
+    return f.astype(np.float32)          # float32-exact initial values
+
+
+CASES = [
+    # name, lattice, grid, viscosity, wall kind, inlet, outlet, bi kind, steps
+    dict(name="d3q19_periodic_uniform_force", lattice="D3Q19", grid=(6, 5, 7),
+         viscosity=0.1, walls=None, faces=("x_min", "x_max"),
+         bi=dict(body_force="uniform"), steps=4),
+    dict(name="d3q19_zwalls_uniform_force", lattice="D3Q19", grid=(5, 6, 8),
+         viscosity=0.1, walls="z", faces=("x_min", "x_max"),
+         bi=dict(body_force="uniform"), steps=4),
+    dict(name="d3q19_random_walls_field_force", lattice="D3Q19", grid=(6, 7, 5),
+         viscosity=0.05, walls="random", faces=("x_min", "x_max"),
+         bi=dict(body_force="field"), steps=3),
+    dict(name="d3q19_zou_he_x", lattice="D3Q19", grid=(8, 4, 6),
+         viscosity=0.1, walls="y", faces=("x_min", "x_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 * 1.01, outlet_pressure=1.0 / 3.0),
+         steps=4),
+    dict(name="d3q19_zou_he_y_min_z_max", lattice="D3Q19", grid=(5, 6, 7),
+         viscosity=0.08, walls="random", faces=("y_min", "z_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 2e-3, outlet_pressure=1.0 / 3.0 - 1e-3,
+                 body_force="uniform"), steps=3),
+    dict(name="d3q19_zou_he_same_face", lattice="D3Q19", grid=(4, 5, 6),
+         viscosity=0.1, walls=None, faces=("z_max", "z_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0),
+         steps=2),
+    dict(name="d3q19_wall_mask_update", lattice="D3Q19", grid=(6, 5, 5),
+         viscosity=0.1, walls="z", faces=("x_min", "x_max"),
+         bi=dict(body_force="uniform", wall_mask_update="random"), steps=3),
+    dict(name="d2q9_periodic_uniform_force", lattice="D2Q9", grid=(7, 6),
+         viscosity=0.1, walls=None, faces=("x_min", "x_max"),
+         bi=dict(body_force="uniform"), steps=5),
+    dict(name="d2q9_channel_zou_he", lattice="D2Q9", grid=(12, 8),
+         viscosity=0.1, walls="y2", faces=("x_min", "x_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 * 1.01, outlet_pressure=1.0 / 3.0),
+         steps=5),
+    dict(name="d2q9_zou_he_y_max_x_min_field", lattice="D2Q9", grid=(9, 7),
+         viscosity=0.07, walls="random", faces=("y_max", "x_min"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0,
+                 body_force="field"), steps=4),
+    # last-axis extents that are multiples of 4 (vectorised kernels), with
+    # rows of one vector, rows longer than a warp, and faces on that axis
+    dict(name="d3q19_vec_faces_on_last_axis", lattice="D3Q19", grid=(4, 5, 12),
+         viscosity=0.1, walls="random", faces=("z_min", "z_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0,
+                 body_force="field"), steps=3),
+    dict(name="d3q19_vec_long_rows", lattice="D3Q19", grid=(3, 3, 136),
+         viscosity=0.1, walls="random", faces=("x_min", "y_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0,
+                 body_force="uniform"), steps=3),
+    dict(name="d3q19_vec_rows_of_4", lattice="D3Q19", grid=(6, 5, 4),
+         viscosity=0.12, walls="z", faces=("z_min", "x_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0),
+         steps=3),
+    dict(name="d2q9_vec_long_rows", lattice="D2Q9", grid=(5, 132),
+         viscosity=0.1, walls="random", faces=("y_min", "y_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0,
+                 body_force="field"), steps=4),
+    dict(name="d2q9_vec_rows_of_4", lattice="D2Q9", grid=(7, 4),
+         viscosity=0.1, walls=None, faces=("x_min", "y_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, body_force="uniform"), steps=3),
+]
+
+
+def _walls(kind, grid, rng):
+    if kind is None:
+        return None
+    w = np.zeros(grid, dtype=bool)
+    if kind == "z":
+        w[..., 0] = True
+        w[..., -1] = True
+    elif kind == "y":
+        w[:, 0, ...] = True
+        w[:, -1, ...] = True
+    elif kind == "y2":
+        w[:, 0] = True
+        w[:, -1] = True
+    elif kind == "random":
+        w = rng.random(grid) < 0.2
+    return w
+
+
+def run_case(lbm, jnp, case, mode, seed):
+    rng = np.random.default_rng(seed + 1000)
+    grid = case["grid"]
+    D = len(grid)
+    walls = _walls(case["walls"], grid, rng)
+    node = lbm.LBMNode(name=case["name"], timestep=1.0, grid_shape=grid,
+                       viscosity=case["viscosity"], lattice=case["lattice"],
+                       wall_mask=walls, inlet_face=case["faces"][0],
+                       outlet_face=case["faces"][1])
+    f0 = _perturbed_f(lbm, node, seed)
+    state = node.initial_state()
+    f_in = f0.astype(np.float64) if mode == "x64" else f0
+    state = {**state, "f": jnp.asarray(f_in)}
+    bi, bi_np = {}, {}
+    for k, v in case["bi"].items():
+        if k == "body_force":
+            if v == "uniform":
+                arr = (np.array([1e-4, -3e-5, 2e-5][:D], dtype=np.float32))
+            else:
+                arr = (1e-4 * rng.standard_normal(grid + (D,))).astype(np.float32)
+            bi[k] = jnp.asarray(arr)
+            bi_np[k] = arr
+        elif k == "wall_mask_update":
+            arr = rng.random(grid) < 0.15
+            bi[k] = jnp.asarray(arr)
+            bi_np[k] = arr
+        else:
+            bi[k] = np.float32(v)
+            bi_np[k] = np.float32(v)
+    out = {"f0": f0, "wall": walls if walls is not None else np.zeros(grid, bool),
+           "tau": np.float64(node.tau)}
+    for k, v in bi_np.items():
+        out["bi_" + k] = np.asarray(v)
+    for step in range(case["steps"]):
+        state = node.update(state, bi, 1.0)
+        if step == 0:
+            for key in ("f", "density", "velocity", "pressure"):
+                out["step1_" + key] = np.asarray(_plain(state[key]))
+    for key in ("f", "density", "velocity", "pressure"):
+        out["final_" + key] = np.asarray(_plain(state[key]))
+    flux = node.compute_boundary_fluxes(state, {}, 1.0)
+    out["final_outlet_pressure_avg"] = np.asarray(_plain(flux["outlet_pressure_avg"]))
+    return out
+
+
+def unit_vectors(lbm, jnp, seed=7):
+    """Golden vectors for the pure kernels on random inputs (x64)."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for lat in (lbm.d3q19(), lbm.d2q9()):
+        tag = lat.name.lower()
+        grid = (4, 3, 5)[: lat.D]
+        rho = 1.0 + 0.01 * rng.standard_normal(grid)
+        u = 0.05 * rng.standard_normal(grid + (lat.D,))
+        F = 1e-3 * rng.standard_normal(grid + (lat.D,))
+        f = rng.random(grid + (lat.Q,))
+        out[f"{tag}_e"] = lat.e
+        out[f"{tag}_w"] = lat.w
+        out[f"{tag}_opp"] = lat.opp
+        out[f"{tag}_rho"] = rho
+        out[f"{tag}_u"] = u
+        out[f"{tag}_F"] = F
+        out[f"{tag}_frand"] = f
+        out[f"{tag}_feq"] = np.asarray(_plain(lbm._equilibrium(jnp.asarray(rho), jnp.asarray(u), lat.e, lat.w, lat.cs2)))
+        d, v = lbm._compute_macroscopic(jnp.asarray(f), lat.e, force=jnp.asarray(F))
+        out[f"{tag}_macro_rho"] = np.asarray(_plain(d))
+        out[f"{tag}_macro_u"] = np.asarray(_plain(v))
+        out[f"{tag}_stream"] = np.asarray(_plain(lbm._stream(jnp.asarray(f), lat.e, lat.D)))
+        out[f"{tag}_guo"] = np.asarray(_plain(lbm._guo_forcing(
+            jnp.asarray(rho), jnp.asarray(u), jnp.asarray(F), 0.73, lat.e, lat.w, lat.cs2)))
+        out[f"{tag}_opp_map"] = lbm._get_opp_map(lat.e)
+        for axis in range(lat.D):
+            for side in ("min", "max"):
+                k, un, t = lbm._classify_directions(lat.e, axis, side)
+                out[f"{tag}_classify_{axis}_{side}"] = np.array(
+                    [len(k), len(un), len(t)] + k + un + t, dtype=np.int32)
+    return out
+
+
+def main(ref_root="/root/reference"):
+    ref_root = Path(ref_root)
+    lbm = _install_shims(ref_root)
+    jnp = sys.modules["jax.numpy"]
+    golden = {}
+    MODE["value"] = "x64"
+    golden.update({f"unit_{k}": v for k, v in unit_vectors(lbm, jnp).items()})
+    for i, case in enumerate(CASES):
+        for mode in ("x64", "f32"):
+            MODE["value"] = mode
+            res = run_case(lbm, jnp, case, mode, seed=i)
+            for k, v in res.items():
+                golden[f"{case['name']}|{mode}|{k}"] = v
+    MODE["value"] = "x64"
+    out = Path(__file__).with_name("lbm_golden.npz")
+    np.savez_compressed(out, **golden)
+    meta = {c["name"]: c for c in CASES}
+    print(f"wrote {out} ({out.stat().st_size / 1024:.1f} KiB, {len(golden)} arrays, "
+          f"{len(meta)} cases)")
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

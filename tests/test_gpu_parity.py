@@ -1,0 +1,216 @@
+"""GPU parity of the sm_100a kernels against the oracle and the reference.
+
+* golden cases (the reference's own lbm.py, executed): per-step ``update``
+  (float32 state between steps, like the reference's float32 path) and
+  fused ``run`` (offsets kept on the device), FP32 and FP64 storage;
+* the 64^3 force-driven channel, 500 steps, FP32 vs the FP64 oracle: relative
+  L2 of density and velocity <= 1e-5;
+* the documented face extensions against the oracle.
+
+Tolerances are written per test.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lbm_ref as R
+from tests.golden.make_golden import CASES
+
+pytestmark = pytest.mark.gpu
+
+F32_EPS = float(np.finfo(np.float32).eps)
+
+
+def _node_for(golden, case, storage="f32"):
+    from maddening_b200 import LBMNode
+    p = f"{case['name']}|x64|"
+    wall = golden[p + "wall"]
+    node = LBMNode(case["name"], 1.0, grid_shape=case["grid"], viscosity=case["viscosity"],
+                   lattice=case["lattice"], wall_mask=wall if wall.any() else None,
+                   inlet_face=case["faces"][0], outlet_face=case["faces"][1], storage=storage)
+    st = node.initial_state()
+    dt = torch.float64 if storage == "f64" else torch.float32
+    st["f"] = torch.as_tensor(golden[p + "f0"].astype(np.float64), device="cuda").to(dt)
+    bi = {}
+    for k in golden.files:
+        if k.startswith(p + "bi_"):
+            name = k[len(p) + 3:]
+            v = golden[k]
+            bi[name] = np.float32(v) if v.ndim == 0 else v
+    return node, st, bi, p
+
+
+def _maxabs(a, b):
+    return float(np.max(np.abs(a.detach().cpu().numpy().astype(np.float64) - b)))
+
+
+def _maxrel(a, b):
+    """Largest |a - b| / |b| (populations are O(1/36 .. 4/9), never near 0)."""
+    a = a.detach().cpu().numpy().astype(np.float64)
+    return float(np.max(np.abs(a - b) / np.abs(b)))
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_update_per_step_matches_reference(golden, case):
+    """One ``update`` per step, float32 state in between (the reference's
+    float32 dtype): within float32 rounding of the x64 reference."""
+    node, st, bi, p = _node_for(golden, case)
+    st = node.update(st, bi, 1.0)
+    assert _maxrel(st["f"], golden[p + "step1_f"]) <= 4 * F32_EPS
+    for key, tol in (("density", 4e-7), ("velocity", 4e-7), ("pressure", 2e-7)):
+        err = _maxabs(st[key], golden[p + "step1_" + key])
+        assert err <= tol, (key, err)
+    for _ in range(case["steps"] - 1):
+        st = node.update(st, bi, 1.0)
+    assert _maxrel(st["f"], golden[p + "final_f"]) <= 8 * F32_EPS
+    for key, tol in (("density", 1e-6), ("velocity", 1e-6), ("pressure", 4e-7)):
+        err = _maxabs(st[key], golden[p + "final_" + key])
+        assert err <= tol, (key, err)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_fused_run_matches_reference(golden, case):
+    node, st, bi, p = _node_for(golden, case)
+    out = node.run(st, bi, case["steps"])
+    assert _maxrel(out["f"], golden[p + "final_f"]) <= 4 * F32_EPS
+    for key, tol in (("density", 4e-7), ("velocity", 4e-7), ("pressure", 2e-7)):
+        err = _maxabs(out[key], golden[p + "final_" + key])
+        assert err <= tol, (key, err)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_fp64_storage_matches_reference_to_1e12(golden, case):
+    node, st, bi, p = _node_for(golden, case, storage="f64")
+    out = node.run(st, bi, case["steps"])
+    assert out["f"].dtype == torch.float64
+    for key in ("f", "density", "velocity", "pressure"):
+        err = _maxabs(out[key], golden[p + "final_" + key])
+        assert err <= 1e-12, (key, err)
+    st1 = node.update(st, bi, 1.0)
+    for key in ("f", "density", "velocity", "pressure"):
+        assert _maxabs(st1[key], golden[p + "step1_" + key]) <= 1e-13
+
+
+def test_channel64_500_steps_fp32_within_1e5_of_fp64(golden):
+    """64^3 channel, z walls, tau 0.8, F = (1e-6, 0, 0), 500 steps: FP32 kernel
+    vs the FP64 oracle, relative L2 of density and velocity <= 1e-5."""
+    from maddening_b200 import LBMNode
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "channel64.npz")
+    ref = np.load(path)
+    lat = R.d3q19()
+    grid = (64, 64, 64)
+    f0, _ = R.channel_state(lat, grid, seed=0)
+    np.testing.assert_array_equal(f0[:2, :2, :2], ref["f0_check"])
+    node = LBMNode("channel", 1.0, grid_shape=grid, viscosity=0.1, wall_mask=R.z_walls(grid))
+    st = node.initial_state()
+    st["f"] = torch.as_tensor(f0, device="cuda")
+    bi = {"body_force": np.array([1e-6, 0.0, 0.0], dtype=np.float32)}
+    out = node.run(st, bi, 500)
+    rho = out["density"].cpu().numpy()
+    u = out["velocity"].cpu().numpy()
+    e_rho = R.rel_l2(rho, ref["x64_rho"])
+    e_u = R.rel_l2(u, ref["x64_u"])
+    rd = out["f"].double().sum(-1).cpu().numpy() - 1.0
+    e_rd = R.rel_l2(rd, ref["x64_rho_dev"])
+    e_u32 = R.rel_l2(u, ref["f32_u"])
+    print(f"\nchannel64 FP32 vs FP64 oracle: relL2 rho={e_rho:.2e} u={e_u:.2e} "
+          f"(rho-1)={e_rd:.2e}; vs float32 reference path: u={e_u32:.2e}")
+    assert e_rho <= 1e-5
+    assert e_u <= 1e-5
+
+
+def _small_obstacle_case(lattice="D3Q19", grid=(16, 8, 12), seed=3):
+    rng = np.random.default_rng(seed)
+    wall = np.zeros(grid, dtype=bool)
+    idx = np.indices(grid)
+    for _ in range(3):
+        c = [rng.uniform(3, grid[0] - 3)] + [rng.uniform(0, n) for n in grid[1:]]
+        r = rng.uniform(1.5, 2.5)
+        d2 = sum((idx[a] - c[a]) ** 2 for a in range(len(grid)))
+        wall |= d2 < r * r
+    wall[0] = False
+    wall[-1] = False
+    return wall
+
+
+@pytest.mark.parametrize("lattice,grid", [("D3Q19", (16, 8, 12)), ("D3Q19", (14, 6, 9)),
+                                          ("D2Q9", (20, 16)), ("D2Q9", (18, 11))])
+@pytest.mark.parametrize("storage", ["f32", "f64"])
+def test_velocity_inlet_zero_gradient_outlet_vs_oracle(lattice, grid, storage):
+    """Extensions (no reference counterpart): velocity inlet at x_min and
+    zero-gradient outlet at x_max, obstacles, 30 steps, vs the FP64 oracle."""
+    from maddening_b200 import LBMNode
+    wall = _small_obstacle_case(lattice, grid)
+    D = len(grid)
+    u_in = np.array([0.05] + [0.0] * (D - 1))
+    orc = R.OracleLBM(grid, 0.1 / 3.0, lattice, wall_mask=wall, outlet_condition="zero_gradient")
+    node = LBMNode("obst", 1.0, grid_shape=grid, viscosity=0.1 / 3.0, lattice=lattice,
+                   wall_mask=wall, outlet_condition="zero_gradient", storage=storage)
+    s_o = orc.initial_state()
+    s_o["f"] = s_o["f"].astype(np.float64)
+    bi = {"inlet_velocity": u_in}
+    for _ in range(30):
+        s_o = orc.update(s_o, bi)
+    st = node.initial_state()
+    out = node.run(st, bi, 30)
+    tol = 1e-12 if storage == "f64" else 2e-6
+    for key in ("f", "density", "velocity"):
+        err = _maxabs(out[key], s_o[key])
+        assert err <= tol, (key, err)
+    one = node.initial_state()
+    for _ in range(3):
+        one = node.update(one, bi, 1.0)
+    s3 = orc.initial_state()
+    s3["f"] = s3["f"].astype(np.float64)
+    for _ in range(3):
+        s3 = orc.update(s3, bi)
+    assert _maxabs(one["velocity"], s3["velocity"]) <= (1e-13 if storage == "f64" else 1e-6)
+
+
+def test_device_resident_boundary_inputs_match_host_values(golden):
+    """Scalars and vectors given as CUDA tensors (traced values) take the
+    device-values path and give the same result as host values."""
+    case = next(c for c in CASES if c["name"] == "d3q19_zou_he_y_min_z_max")
+    node, st, bi, p = _node_for(golden, case)
+    host = node.run(st, bi, 3)
+    bi_dev = {k: torch.as_tensor(np.asarray(v), device="cuda") for k, v in bi.items()}
+    dev = node.run(st, bi_dev, 3)
+    for key in ("f", "density", "velocity"):
+        assert torch.equal(host[key], dev[key]), key
+
+
+@pytest.mark.parametrize("storage,tol_u", [("f16", 2e-2), ("bf16", 1e-1)])
+def test_reduced_precision_storage_close_to_fp64(storage, tol_u):
+    """FP16/BF16 normalised offsets with FP32 arithmetic: obstacle flow with a
+    velocity inlet (u = 0.05), 200 steps, relative L2 error vs FP64 storage."""
+    from maddening_b200 import LBMNode
+    grid = (32, 16, 16)
+    wall = _small_obstacle_case("D3Q19", grid, seed=5)
+    bi = {"inlet_velocity": np.array([0.05, 0.0, 0.0])}
+    ref = LBMNode("r", 1.0, grid_shape=grid, viscosity=0.1 / 3, wall_mask=wall,
+                  outlet_condition="zero_gradient", storage="f64")
+    low = LBMNode("l", 1.0, grid_shape=grid, viscosity=0.1 / 3, wall_mask=wall,
+                  outlet_condition="zero_gradient", storage=storage)
+    a = ref.run(ref.initial_state(), bi, 200)
+    b = low.run(low.initial_state(), bi, 200)
+    e_u = R.rel_l2(b["velocity"].cpu().numpy(), a["velocity"].cpu().numpy())
+    e_rho = R.rel_l2(b["density"].cpu().numpy(), a["density"].cpu().numpy())
+    print(f"\n{storage}: relL2 u={e_u:.2e} rho={e_rho:.2e}")
+    assert e_u <= tol_u
+    assert e_rho <= 1e-3
+
+
+def test_mass_momentum_fp64_reduction():
+    from maddening_b200 import LBMNode
+    grid = (24, 20, 36)
+    node = LBMNode("m", 1.0, grid_shape=grid)
+    rng = np.random.default_rng(1)
+    f = (node.lattice.w * (1 + 1e-2 * rng.standard_normal(grid + (19,)))).astype(np.float32)
+    out = node.mass_momentum(torch.as_tensor(f, device="cuda")).cpu().numpy()
+    f64 = f.astype(np.float64)
+    mass = f64.sum()
+    mom = f64.reshape(-1, 19).sum(axis=0) @ node.lattice.e.astype(np.float64)
+    assert abs(out[0] - mass) <= 1e-9 * mass
+    np.testing.assert_allclose(out[1:], mom, rtol=1e-9, atol=1e-9)
