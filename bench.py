@@ -296,7 +296,6 @@ def run_ours(args):
 
     if rank == 0:
         peak, peak_kind = _peaks()
-        achieved = BYTES_PER_CELL * cells * K / (t_dev / world * world) / 1e9 / 1.0
         achieved = BYTES_PER_CELL * (cells * K) / t_dev / 1e9  # per GPU
         line = {
             "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS",
@@ -312,7 +311,7 @@ def run_ours(args):
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_source": peak_kind, "traffic": None,
                          "bytes_per_cell": BYTES_PER_CELL,
-                         "kernel": "k_step<19,float,4,0> (fused pull-stream-collide)"},
+                         "kernel": "k_step<19,float,1,0> (fused pull-stream-collide)"},
             "e2e": {"value": round(world * cells * K / t_e2e / 1e6, 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
                     "note": "LBMNode.run with pinned-host state in/out, per K-step rollout"},
@@ -368,7 +367,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--grid", type=int, default=256,
+                    help="cube side (256 = the benchmark workload; smaller for profiling)")
     args = ap.parse_args()
+    global GRID
+    GRID = (args.grid,) * 3
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -246,10 +246,10 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
   }
   int vv = 4;
   switch (p->storage) {
-    case LBM_STORE_F32: p->elem = 4; p->io = 4; vv = 4; break;
+    case LBM_STORE_F32: p->elem = 4; p->io = 4; vv = lbm::StoreT<float>::V; break;
     case LBM_STORE_F16:
-    case LBM_STORE_BF16: p->elem = 2; p->io = 4; vv = 4; break;
-    case LBM_STORE_F64: p->elem = 8; p->io = 8; vv = 2; break;
+    case LBM_STORE_BF16: p->elem = 2; p->io = 4; vv = lbm::StoreT<__half>::V; break;
+    case LBM_STORE_F64: p->elem = 8; p->io = 8; vv = lbm::StoreT<double>::V; break;
   }
   p->V = (dims[2] % vv == 0) ? vv : 1;
   p->g.n0 = static_cast<int>(dims[0]);

@@ -40,32 +40,45 @@ namespace lbm {
 
 template <class S>
 struct StoreT;
+// Cells per thread on the step path, per storage form.  One cell per thread
+// at 128 threads x 8 blocks per SM (<= 64 registers, 32 warps resident)
+// measured fastest on B200 for every form; wider forms need more registers
+// than a full SM of warps can hold.
+#ifndef LBM_F32_VEC
+#define LBM_F32_VEC 1
+#endif
+#ifndef LBM_F16_VEC
+#define LBM_F16_VEC 1
+#endif
+#ifndef LBM_F64_VEC
+#define LBM_F64_VEC 1
+#endif
 template <>
 struct StoreT<float> {
   using R = float;   // arithmetic type
   using IO = float;  // type of f / force / moment buffers at the ABI
-  static constexpr int V = 4;
+  static constexpr int V = LBM_F32_VEC;
   static constexpr bool kScaled = false;
 };
 template <>
 struct StoreT<__half> {
   using R = float;
   using IO = float;
-  static constexpr int V = 4;
+  static constexpr int V = LBM_F16_VEC;
   static constexpr bool kScaled = true;
 };
 template <>
 struct StoreT<__nv_bfloat16> {
   using R = float;
   using IO = float;
-  static constexpr int V = 4;
+  static constexpr int V = LBM_F16_VEC;
   static constexpr bool kScaled = true;
 };
 template <>
 struct StoreT<double> {
   using R = double;
   using IO = double;
-  static constexpr int V = 2;
+  static constexpr int V = LBM_F64_VEC;
   static constexpr bool kScaled = false;
 };
 
@@ -114,6 +127,16 @@ struct VIO<float, 4> {
   }
   __device__ __forceinline__ static void st(float* p, const float (&v)[4]) {
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <>
+struct VIO<float, 2> {
+  __device__ __forceinline__ static void ld(const float* p, float (&o)[2]) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    o[0] = v.x; o[1] = v.y;
+  }
+  __device__ __forceinline__ static void st(float* p, const float (&v)[2]) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
   }
 };
 template <>
@@ -462,7 +485,16 @@ __device__ __forceinline__ void face_zero_gradient(typename StoreT<S>::R (&f)[Q]
 // Kernels
 // ---------------------------------------------------------------------------
 
-constexpr int kBlock = 256;
+// Launch shape of the step kernels (threads per block, minimum resident
+// blocks per SM for the register budget); overridable at compile time.
+#ifndef LBM_STEP_BLOCK
+#define LBM_STEP_BLOCK 128
+#endif
+#ifndef LBM_STEP_MINB
+#define LBM_STEP_MINB 8
+#endif
+constexpr int kBlock = LBM_STEP_BLOCK;
+constexpr int kMinBlocks = LBM_STEP_MINB;
 
 enum StepMode : int { kOutState = 0, kOutAoS = 1 };
 
@@ -608,7 +640,7 @@ __global__ void __launch_bounds__(kBlock) k_prepare(const StepArgs a) {
 // One fused step: pull p -> wall swap -> faces (= reference f_bc) -> moments
 // (reference outputs) -> collide (next p) or write f_bc (MODE kOutAoS).
 template <int Q, class S, int V, int MODE>
-__global__ void __launch_bounds__(kBlock) k_step(const StepArgs a) {
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_step(const StepArgs a) {
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
   const Geo& g = a.g;
