@@ -206,7 +206,10 @@ def run_ours(args):
     cells = GRID[0] * GRID[1] * GRID[2]
     wall = random_spheres(GRID, seed=0)
     node = LBMNode("bench", 1.0, grid_shape=GRID, viscosity=(TAU - 0.5) / 3.0,
-                   wall_mask=wall, outlet_condition="zero_gradient", device=dev)
+                   wall_mask=wall, outlet_condition="zero_gradient", device=dev,
+                   storage=args.storage)
+    io_dtype = torch.float64 if args.storage == "f64" else torch.float32
+    bytes_per_cell = {"f32": 152, "f16": 76, "bf16": 76, "f64": 304}[args.storage]
     bi = {"inlet_velocity": np.array(U_IN)}
 
     # device-resident buffers for the kernel-throughput number
@@ -216,9 +219,9 @@ def run_ours(args):
     plan = node.plan
     ws = torch.empty(plan.workspace_bytes(), dtype=torch.uint8, device=dev)
     sargs, keep = node._step_args(st, bi, dev)
-    rho = torch.empty(GRID, device=dev)
-    vel = torch.empty(GRID + (3,), device=dev)
-    prs = torch.empty(GRID, device=dev)
+    rho = torch.empty(GRID, device=dev, dtype=io_dtype)
+    vel = torch.empty(GRID + (3,), device=dev, dtype=io_dtype)
+    prs = torch.empty(GRID, device=dev, dtype=io_dtype)
     mom = _lib.lbm_moments()
     mom.density, mom.velocity, mom.pressure = rho.data_ptr(), vel.data_ptr(), prs.data_ptr()
     lib = _lib.lib()
@@ -248,7 +251,7 @@ def run_ours(args):
     # e2e: public API, state in pinned host memory
     f_host = f_a.cpu().pin_memory()
     wall_host = torch.as_tensor(wall.astype(np.uint8)).pin_memory()
-    outs = {k: torch.empty(s, dtype=torch.float32).pin_memory() for k, s in
+    outs = {k: torch.empty(s, dtype=io_dtype).pin_memory() for k, s in
             (("f", GRID + (19,)), ("density", GRID), ("velocity", GRID + (3,)),
              ("pressure", GRID))}
     state_host = {"f": f_host, "wall_mask": wall_host}
@@ -269,8 +272,8 @@ def run_ours(args):
     e3.record(stream)
     _barrier(world)
     t_e2e = _max_over_ranks(world, e2.elapsed_time(e3) / 1e3)
-    h2d = f_host.numel() * 4 + wall_host.numel()
-    d2h = sum(v.numel() * 4 for v in outs.values())
+    h2d = f_host.numel() * f_host.element_size() + wall_host.numel()
+    d2h = sum(v.numel() * v.element_size() for v in outs.values())
 
     # variants: other storage forms of the same workload (informational)
     variants = {}
@@ -296,22 +299,24 @@ def run_ours(args):
 
     if rank == 0:
         peak, peak_kind = _peaks()
-        achieved = BYTES_PER_CELL * (cells * K) / t_dev / 1e9  # per GPU
+        achieved = bytes_per_cell * (cells * K) / t_dev / 1e9  # per GPU
         line = {
             "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS",
             "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": round(t_dev / K * 1e3, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.storage == "f64" else "f32",
             "data": "synthetic (seeded spheres, rng seed 0)",
             "config": {"workload": WORKLOAD, "grid": list(GRID), "lattice": "D3Q19",
-                       "storage": "f32 offsets", "tau": TAU, "solid_fraction": float(wall.mean()),
+                       "storage": f"{args.storage} offsets", "tau": TAU, "solid_fraction": float(wall.mean()),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "state 2 x 1.27 GB > 126 MB L2; no flush needed"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "peak_source": peak_kind, "traffic": None,
-                         "bytes_per_cell": BYTES_PER_CELL,
-                         "kernel": "k_step<19,float,1,0> (fused pull-stream-collide)"},
+                         "bytes_per_cell": bytes_per_cell,
+                         "kernel": "k_step<19,float,0,true,false> (fused pull-stream-collide, "
+                                   "faces on)"},
             "e2e": {"value": round(world * cells * K / t_e2e / 1e6, 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
                     "note": "LBMNode.run with pinned-host state in/out, per K-step rollout"},
@@ -367,6 +372,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--storage", choices=["f32", "f16", "bf16", "f64"], default="f32",
+                    help="population storage of the measured run (default f32)")
     ap.add_argument("--grid", type=int, default=256,
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
     args = ap.parse_args()

@@ -14,8 +14,7 @@
 struct lbm_plan {
   int Q = 0, D = 0, storage = 0;
   int64_t shape[3] = {0, 0, 0};  // reference grid_shape
-  lbm::Geo g{};                  // internal geometry (V-dependent nq / nvec)
-  int V = 1;                     // cells per thread on the step path
+  lbm::Geo g{};                  // internal geometry
   double tau = 0;
   size_t elem = 4;               // bytes per stored population
   size_t io = 4;                 // bytes per f / force / moment element
@@ -42,6 +41,37 @@ int cuda_check(cudaError_t e, const char* what) {
 
 size_t state_bytes(const lbm_plan* p) {
   return static_cast<size_t>(p->Q) * static_cast<size_t>(p->g.ncell) * p->elem;
+}
+
+// Multiply-high constants for x / d, 0 <= x < 2^31 (see lbm::fdiv).
+lbm::FastDiv make_fastdiv(uint32_t d) {
+  lbm::FastDiv f;
+  f.d = d;
+  uint32_t s = 0;
+  while ((uint64_t(1) << s) < d) ++s;
+  f.s = s;
+  f.m = static_cast<uint32_t>(((uint64_t(1) << 32) * ((uint64_t(1) << s) - d)) / d + 1);
+  return f;
+}
+
+uint32_t host_fdiv(uint32_t x, const lbm::FastDiv& f) {
+  const uint32_t hi = static_cast<uint32_t>((static_cast<uint64_t>(x) * f.m) >> 32);
+  return (hi + x) >> f.s;
+}
+
+bool fastdiv_ok(const lbm::FastDiv& f, uint32_t xmax) {
+  const uint32_t probes[] = {0u, 1u, f.d - 1, f.d, f.d + 1, 2 * f.d - 1, 2 * f.d,
+                             xmax / 2, xmax - 1, xmax};
+  for (uint32_t x : probes)
+    if (x <= xmax && host_fdiv(x, f) != x / f.d) return false;
+  return true;
+}
+
+// Population plane pointers of a state buffer.
+void planes(const lbm_plan* p, const void* base, const void** out) {
+  const char* b = static_cast<const char*>(base);
+  for (int q = 0; q < p->Q; ++q)
+    out[q] = b + static_cast<size_t>(q) * p->g.ncell * p->elem;
 }
 
 // Maps one face condition of the ABI to the kernel form (internal axes).
@@ -115,64 +145,72 @@ int build_args(const lbm_plan* p, const lbm_step_args* args, const lbm_moments* 
 
 unsigned grid_for(uint64_t n) { return static_cast<unsigned>((n + lbm::kBlock - 1) / lbm::kBlock); }
 
-template <int Q, class S, int V>
+template <int Q, class S>
 int launch_prepare(const lbm::StepArgs& a, cudaStream_t s) {
-  lbm::k_prepare<Q, S, V><<<grid_for(a.g.nvec), lbm::kBlock, 0, s>>>(a);
+  const unsigned grid = grid_for(a.g.ncell);
+  if (a.force_mode != 0)
+    lbm::k_prepare<Q, S, true><<<grid, lbm::kBlock, 0, s>>>(a);
+  else
+    lbm::k_prepare<Q, S, false><<<grid, lbm::kBlock, 0, s>>>(a);
   return cuda_check(cudaGetLastError(), "k_prepare launch");
 }
 
-template <int Q, class S, int V>
+template <int Q, class S, int MODE>
+void launch_step_mode(const lbm::StepArgs& a, cudaStream_t s) {
+  const unsigned grid = grid_for(a.g.ncell);
+  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (faces) {
+    if (force) lbm::k_step<Q, S, MODE, true, true><<<grid, lbm::kBlock, 0, s>>>(a);
+    else lbm::k_step<Q, S, MODE, true, false><<<grid, lbm::kBlock, 0, s>>>(a);
+  } else {
+    if (force) lbm::k_step<Q, S, MODE, false, true><<<grid, lbm::kBlock, 0, s>>>(a);
+    else lbm::k_step<Q, S, MODE, false, false><<<grid, lbm::kBlock, 0, s>>>(a);
+  }
+}
+
+template <int Q, class S>
 int launch_step(const lbm::StepArgs& a, bool final_aos, cudaStream_t s) {
-  if (final_aos)
-    lbm::k_step<Q, S, V, lbm::kOutAoS><<<grid_for(a.g.nvec), lbm::kBlock, 0, s>>>(a);
-  else
-    lbm::k_step<Q, S, V, lbm::kOutState><<<grid_for(a.g.nvec), lbm::kBlock, 0, s>>>(a);
+  if (final_aos) launch_step_mode<Q, S, lbm::kOutAoS>(a, s);
+  else launch_step_mode<Q, S, lbm::kOutState>(a, s);
   return cuda_check(cudaGetLastError(), "k_step launch");
 }
 
 // Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies.
-template <int Q, class S, int V>
+template <int Q, class S>
 int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
               int64_t n, char* ws) {
   const size_t sb = state_bytes(p);
-  void* A = ws;
-  void* B = ws + sb;
+  char* A = ws;
+  char* B = ws + sb;
   a.f_in = f_in;
-  a.pout = A;
-  int rc = launch_prepare<Q, S, V>(a, s);
+  planes(p, A, const_cast<const void**>(a.pout));
+  int rc = launch_prepare<Q, S>(a, s);
   if (rc) return rc;
   lbm::StepArgs m = a;  // intermediate steps write no moments
   m.rho = m.vel = m.prs = nullptr;
   for (int64_t i = 0; i + 1 < n; ++i) {
-    m.pin = A;
-    m.pout = B;
-    rc = launch_step<Q, S, V>(m, false, s);
+    planes(p, A, m.pin);
+    planes(p, B, const_cast<const void**>(m.pout));
+    rc = launch_step<Q, S>(m, false, s);
     if (rc) return rc;
-    void* t = A;
+    char* t = A;
     A = B;
     B = t;
   }
-  a.pin = A;
+  planes(p, A, a.pin);
   a.f_out = f_out;
-  return launch_step<Q, S, V>(a, true, s);
-}
-
-template <int Q, class S>
-int dispatch_v(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a, const void* f_in,
-               void* f_out, int64_t n, char* ws) {
-  constexpr int VV = lbm::StoreT<S>::V;
-  if (p->V == VV) return run_steps<Q, S, VV>(p, s, a, f_in, f_out, n, ws);
-  return run_steps<Q, S, 1>(p, s, a, f_in, f_out, n, ws);
+  return launch_step<Q, S>(a, true, s);
 }
 
 template <int Q>
 int dispatch_s(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a, const void* f_in,
                void* f_out, int64_t n, char* ws) {
   switch (p->storage) {
-    case LBM_STORE_F32: return dispatch_v<Q, float>(p, s, a, f_in, f_out, n, ws);
-    case LBM_STORE_F16: return dispatch_v<Q, __half>(p, s, a, f_in, f_out, n, ws);
-    case LBM_STORE_BF16: return dispatch_v<Q, __nv_bfloat16>(p, s, a, f_in, f_out, n, ws);
-    case LBM_STORE_F64: return dispatch_v<Q, double>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_F32: return run_steps<Q, float>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_F16: return run_steps<Q, __half>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_BF16: return run_steps<Q, __nv_bfloat16>(p, s, a, f_in, f_out, n, ws);
+    case LBM_STORE_F64: return run_steps<Q, double>(p, s, a, f_in, f_out, n, ws);
   }
   return fail(LBM_ERR_INVALID, "bad storage");
 }
@@ -240,24 +278,28 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
     dims[0] = 1; dims[1] = p->shape[0]; dims[2] = p->shape[1];
   }
   const int64_t ncell = dims[0] * dims[1] * dims[2];
-  if (ncell >= (int64_t(1) << 32) - 1024) {
+  if (ncell >= (int64_t(1) << 31)) {
     delete p;
     return fail(LBM_ERR_INVALID, "lattice of %lld cells is too large", (long long)ncell);
   }
-  int vv = 4;
   switch (p->storage) {
-    case LBM_STORE_F32: p->elem = 4; p->io = 4; vv = lbm::StoreT<float>::V; break;
+    case LBM_STORE_F32: p->elem = 4; p->io = 4; break;
     case LBM_STORE_F16:
-    case LBM_STORE_BF16: p->elem = 2; p->io = 4; vv = lbm::StoreT<__half>::V; break;
-    case LBM_STORE_F64: p->elem = 8; p->io = 8; vv = lbm::StoreT<double>::V; break;
+    case LBM_STORE_BF16: p->elem = 2; p->io = 4; break;
+    case LBM_STORE_F64: p->elem = 8; p->io = 8; break;
   }
-  p->V = (dims[2] % vv == 0) ? vv : 1;
-  p->g.n0 = static_cast<int>(dims[0]);
-  p->g.n1 = static_cast<int>(dims[1]);
-  p->g.n2 = static_cast<int>(dims[2]);
-  p->g.nq = static_cast<int>(dims[2] / p->V);
-  p->g.nvec = static_cast<uint32_t>(dims[0] * dims[1] * p->g.nq);
-  p->g.ncell = ncell;
+  p->g.n0 = static_cast<uint32_t>(dims[0]);
+  p->g.n1 = static_cast<uint32_t>(dims[1]);
+  p->g.n2 = static_cast<uint32_t>(dims[2]);
+  p->g.plane = static_cast<uint32_t>(dims[1] * dims[2]);
+  p->g.ncell = static_cast<uint32_t>(ncell);
+  p->g.div_n2 = make_fastdiv(p->g.n2);
+  p->g.div_n1 = make_fastdiv(p->g.n1);
+  if (!fastdiv_ok(p->g.div_n2, p->g.ncell) ||
+      !fastdiv_ok(p->g.div_n1, static_cast<uint32_t>(dims[0] * dims[1]))) {
+    delete p;
+    return fail(LBM_ERR_INVALID, "internal: index division constants failed self-check");
+  }
   *plan = p;
   return LBM_OK;
 }
@@ -283,7 +325,7 @@ int lbm_equilibrium(const lbm_plan* p, lbm_stream_t stream, const void* rho, con
                     void* f_out) {
   if (p == nullptr || f_out == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const unsigned grid = grid_for(static_cast<uint64_t>(p->g.ncell));
+  const unsigned grid = grid_for(p->g.ncell);
   if (p->io == 8) {
     if (p->Q == 19)
       lbm::k_equilibrium<19, double><<<grid, lbm::kBlock, 0, s>>>(
@@ -338,23 +380,23 @@ int lbm_mass_momentum(const lbm_plan* p, lbm_stream_t stream, const void* f, dou
   const double nc = static_cast<double>(p->g.ncell);
   if (p->io == 8) {
     if (p->Q == 19) {
-      lbm::k_mass_momentum_part<19, double><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+      lbm::k_mass_momentum_part<19, double><<<kReduceBlocks, lbm::kReduceThreads, 0, s>>>(
           p->g, static_cast<const double*>(f), part);
-      lbm::k_mass_momentum_final<19><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+      lbm::k_mass_momentum_final<19><<<1, lbm::kReduceThreads, 0, s>>>(part, kReduceBlocks, nc, out_dev);
     } else {
-      lbm::k_mass_momentum_part<9, double><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+      lbm::k_mass_momentum_part<9, double><<<kReduceBlocks, lbm::kReduceThreads, 0, s>>>(
           p->g, static_cast<const double*>(f), part);
-      lbm::k_mass_momentum_final<9><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+      lbm::k_mass_momentum_final<9><<<1, lbm::kReduceThreads, 0, s>>>(part, kReduceBlocks, nc, out_dev);
     }
   } else {
     if (p->Q == 19) {
-      lbm::k_mass_momentum_part<19, float><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+      lbm::k_mass_momentum_part<19, float><<<kReduceBlocks, lbm::kReduceThreads, 0, s>>>(
           p->g, static_cast<const float*>(f), part);
-      lbm::k_mass_momentum_final<19><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+      lbm::k_mass_momentum_final<19><<<1, lbm::kReduceThreads, 0, s>>>(part, kReduceBlocks, nc, out_dev);
     } else {
-      lbm::k_mass_momentum_part<9, float><<<kReduceBlocks, lbm::kBlock, 0, s>>>(
+      lbm::k_mass_momentum_part<9, float><<<kReduceBlocks, lbm::kReduceThreads, 0, s>>>(
           p->g, static_cast<const float*>(f), part);
-      lbm::k_mass_momentum_final<9><<<1, lbm::kBlock, 0, s>>>(part, kReduceBlocks, nc, out_dev);
+      lbm::k_mass_momentum_final<9><<<1, lbm::kReduceThreads, 0, s>>>(part, kReduceBlocks, nc, out_dev);
     }
   }
   return cuda_check(cudaGetLastError(), "k_mass_momentum launch");
