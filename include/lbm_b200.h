@@ -148,6 +148,31 @@ int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
                 void* f_out, int64_t n_steps, const lbm_step_args* args,
                 const lbm_moments* out, void* workspace, size_t workspace_bytes);
 
+/* Scratch capacity of lbm_update_noalloc: one population copy of at most
+ * 24 MiB.  D3Q19: up to 331,129 cells with FP32 storage (e.g. 64^3), 662,258
+ * with FP16/BF16, 165,564 with FP64; D2Q9: up to 699,050 cells with FP32. */
+#define LBM_NOALLOC_SCRATCH_BYTES (24u << 20)
+
+/* lbm_update for callers that cannot allocate device memory.  No counterpart in
+ * the reference.  Some callers cannot call cudaMalloc or hand over a workspace:
+ * a custom-call handler whose runtime gives it no scratch allocator, an
+ * embedded or real-time loop where device allocation is not allowed, a plugin
+ * that must not grow its host process's device memory per call.  This entry
+ * point takes no workspace: its
+ * scratch is a static device array of LBM_NOALLOC_SCRATCH_BYTES inside the
+ * library, which every GPU that loads the library holds until the process
+ * exits.  It allocates nothing (no cudaMalloc / cudaFree / allocating library
+ * call).  Its first call on a device looks up that array's device address with
+ * the device current, so make the first call on each device before any stream
+ * capture.  Lattices whose populations need more than the array are rejected
+ * with LBM_ERR_WORKSPACE.  All calls share the one array: calls that overlap on
+ * the GPU (different streams, or different threads without ordering) race and
+ * corrupt each other; order them on one stream.  The array keeps the last
+ * call's contents; nothing in it needs to start at zero (every byte read is
+ * written first in the same call).  Results equal lbm_update's. */
+int lbm_update_noalloc(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+                       void* f_out, const lbm_step_args* args, const lbm_moments* out);
+
 /* Scratch bytes of lbm_mass_momentum. */
 int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes);
 

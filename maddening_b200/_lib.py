@@ -24,6 +24,7 @@ FORCE_NONE, FORCE_UNIFORM, FORCE_FIELD = 0, 1, 2
 FACES = {"x_min": 0, "x_max": 1, "y_min": 2, "y_max": 3, "z_min": 4, "z_max": 5}
 BC_NONE, BC_PRESSURE, BC_VELOCITY, BC_ZERO_GRADIENT = 0, 1, 2, 3
 MOMENTS_DENSITY_DEVIATION = 1
+NOALLOC_SCRATCH_BYTES = 24 << 20  # LBM_NOALLOC_SCRATCH_BYTES
 
 
 class LbmError(RuntimeError):
@@ -68,6 +69,8 @@ _SIGS = {
                     _P, C.c_size_t], C.c_int),
     "lbm_rollout": ([_P, _P, _P, _P, C.c_int64, C.POINTER(lbm_step_args),
                      C.POINTER(lbm_moments), _P, C.c_size_t], C.c_int),
+    "lbm_update_noalloc": ([_P, _P, _P, _P, C.POINTER(lbm_step_args),
+                            C.POINTER(lbm_moments)], C.c_int),
     "lbm_reduce_workspace_bytes": ([_P, C.POINTER(C.c_size_t)], C.c_int),
     "lbm_mass_momentum": ([_P, _P, _P, _P, _P, C.c_size_t], C.c_int),
 }

@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/lbm_b200.h"
@@ -238,6 +239,38 @@ constexpr int kReduceBlocks = 148 * 4;
 
 }  // namespace
 
+// Scratch of lbm_update_noalloc: one population copy, in the module's static
+// device memory (every GPU that loads the library holds it until exit).  In
+// host code this name is a host-side stand-in, not a device address; the
+// device address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LBM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device; looked up on the
+// first call per device (that device current), then cached.
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= kMaxDevices) return fail(LBM_ERR_UNSUPPORTED, "device %d", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    rc = cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    if (rc) return rc;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return LBM_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int lbm_abi_version(void) { return LBM_ABI_VERSION; }
@@ -359,6 +392,21 @@ int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, voi
                 void* workspace, size_t workspace_bytes) {
   return do_steps(plan, stream, f_in, f_out, n_steps, args, out, workspace, workspace_bytes,
                   n_steps > 1 ? 2 : 1);
+}
+
+int lbm_update_noalloc(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+                       void* f_out, const lbm_step_args* args, const lbm_moments* out) {
+  if (plan == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
+  const size_t need = state_bytes(plan);
+  if (need > LBM_NOALLOC_SCRATCH_BYTES)
+    return fail(LBM_ERR_WORKSPACE,
+                "lbm_update_noalloc: this lattice needs %zu bytes of scratch, more than the "
+                "%u-byte static array; use lbm_update with a workspace",
+                need, static_cast<unsigned>(LBM_NOALLOC_SCRATCH_BYTES));
+  void* ws = nullptr;
+  const int rc = noalloc_scratch(&ws);
+  if (rc) return rc;
+  return do_steps(plan, stream, f_in, f_out, 1, args, out, ws, LBM_NOALLOC_SCRATCH_BYTES, 1);
 }
 
 int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes) {
