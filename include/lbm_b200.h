@@ -46,9 +46,9 @@ typedef enum {
 
 typedef enum { LBM_D2Q9 = 9, LBM_D3Q19 = 19 } lbm_lattice;
 
-/* How populations are kept on the device between steps.  All forms store
- * offsets g_q = f_q - w_q (F16/BF16: normalised, g_q / w_q) and do the
- * collide arithmetic in FP32 (FP64 for LBM_STORE_F64). */
+/* How populations are kept on the device between steps.  All forms store the
+ * normalised offsets d_q = (f_q - w_q) / w_q and do the collide arithmetic in
+ * FP32 (FP64 for LBM_STORE_F64). */
 typedef enum {
   LBM_STORE_F32 = 0,
   LBM_STORE_F16 = 1,
