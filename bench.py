@@ -297,6 +297,9 @@ def run_ours(args):
                                  "bytes_per_cell": 76}
             del vn, vs
 
+    if not args.no_variants and rank == 0:
+        variants["adjoint"] = adjoint_cost(dev)
+
     if rank == 0:
         peak, peak_kind = _peaks()
         achieved = bytes_per_cell * (cells * K) / t_dev / 1e9  # per GPU
@@ -335,6 +338,46 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def adjoint_cost(dev):
+    """Cost of the differentiated rollout against the plain forward: 128^3 D3Q19,
+    z walls, tau 0.7, force field 1e-6 N(0,1), 1000 steps, checkpoint every 32,
+    loss = final kinetic energy (FP32 storage)."""
+    import torch
+    from maddening_b200 import LBMNode
+    from oracle import lbm_ref as R  # z-wall mask helper only
+    grid, steps, K = (128, 128, 128), 1000, 32
+    rng = np.random.default_rng(0)
+    node = LBMNode("adj", 1.0, grid_shape=grid, viscosity=0.2 / 3.0, wall_mask=R.z_walls(grid),
+                   device=dev)
+    st = node.initial_state()
+    F = torch.tensor(1e-6 * rng.standard_normal(grid + (3,)), dtype=torch.float32, device=dev,
+                     requires_grad=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    node.run(st, {"body_force": F.detach()}, 10)
+    torch.cuda.synchronize()
+    ev[0].record()
+    node.run(st, {"body_force": F.detach()}, steps)
+    ev[1].record()
+    ev[2].record()
+    out = node.rollout(st, {"body_force": F}, steps, checkpoint_every=K)
+    loss = 0.5 * (out["density"] * (out["velocity"] ** 2).sum(-1)).sum()
+    ev[3].record()
+    ev[4].record()
+    loss.backward()
+    ev[5].record()
+    torch.cuda.synchronize()
+    t_plain = ev[0].elapsed_time(ev[1])
+    t_fwd = ev[2].elapsed_time(ev[3])
+    t_bwd = ev[4].elapsed_time(ev[5])
+    return {"workload": "128^3 D3Q19, z walls, tau 0.7, force field, 1000 steps, "
+                        "checkpoint every 32, FP32",
+            "plain_forward_ms": round(t_plain, 2), "checkpointed_forward_ms": round(t_fwd, 2),
+            "backward_ms": round(t_bwd, 2),
+            "backward_over_forward": round(t_bwd / t_plain, 3),
+            "forward_plus_backward_over_forward": round((t_fwd + t_bwd) / t_plain, 3),
+            "workspace_gb": round(node.plan.adjoint_workspace_bytes(steps, K) / 1e9, 2)}
 
 
 def run_reference(args):

@@ -148,6 +148,36 @@ int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
                 void* f_out, int64_t n_steps, const lbm_step_args* args,
                 const lbm_moments* out, void* workspace, size_t workspace_bytes);
 
+/* ---- Differentiated rollout --------------------------------------------
+ * Reverse mode of lbm_rollout for walls and body forces (no face conditions),
+ * FP32 or FP64 storage.  The reference differentiates LBMNode.update with
+ * jax.grad through lax.scan (graph_manager.py:2697-2805); here the forward keeps
+ * a checkpoint of the populations every `checkpoint_every` steps (<= 0: the
+ * ceiling of sqrt(n_steps)) in the workspace, and the backward recomputes each
+ * segment storing only (rho, u) per step, then runs the hand-written adjoint
+ * step.  The workspace must stay untouched between the two calls. */
+int lbm_adjoint_workspace_bytes(const lbm_plan* plan, int64_t n_steps, int64_t checkpoint_every,
+                                size_t* bytes);
+
+/* Same result as lbm_rollout (f_out, moments of the last step), plus the
+ * checkpoints the backward needs.  f_in must not alias f_out. */
+int lbm_rollout_forward(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, void* f_out,
+                        int64_t n_steps, int64_t checkpoint_every, const lbm_step_args* args,
+                        const lbm_moments* out, void* workspace, size_t workspace_bytes);
+
+/* Gradients of a loss L given dL/d(outputs of the last step): grad_density
+ * (grid), grad_velocity ((grid, D); velocity is 0 in walls), grad_f ((grid, Q));
+ * any may be NULL (= 0).  Outputs (NULL = not wanted): grad_force in FP64 --
+ * (grid, D) for LBM_FORCE_FIELD and LBM_FORCE_NONE (the gradient with respect
+ * to a body-force field, at its value), D values for LBM_FORCE_UNIFORM -- and
+ * grad_f_in = dL/df_in ((grid, Q), the plan's IO type).  f_in, n_steps,
+ * checkpoint_every and args must be the forward's. */
+int lbm_rollout_backward(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+                         int64_t n_steps, int64_t checkpoint_every, const lbm_step_args* args,
+                         const void* grad_density, const void* grad_velocity, const void* grad_f,
+                         double* grad_force, void* grad_f_in, void* workspace,
+                         size_t workspace_bytes);
+
 /* Scratch capacity of lbm_update_noalloc: one population copy of at most
  * 24 MiB.  D3Q19: up to 331,129 cells with FP32 storage (e.g. 64^3), 662,258
  * with FP16/BF16, 165,564 with FP64; D2Q9: up to 699,050 cells with FP32. */

@@ -71,6 +71,12 @@ _SIGS = {
                      C.POINTER(lbm_moments), _P, C.c_size_t], C.c_int),
     "lbm_update_noalloc": ([_P, _P, _P, _P, C.POINTER(lbm_step_args),
                             C.POINTER(lbm_moments)], C.c_int),
+    "lbm_adjoint_workspace_bytes": ([_P, C.c_int64, C.c_int64, C.POINTER(C.c_size_t)],
+                                    C.c_int),
+    "lbm_rollout_forward": ([_P, _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(lbm_step_args),
+                             C.POINTER(lbm_moments), _P, C.c_size_t], C.c_int),
+    "lbm_rollout_backward": ([_P, _P, _P, C.c_int64, C.c_int64, C.POINTER(lbm_step_args),
+                              _P, _P, _P, _P, _P, _P, C.c_size_t], C.c_int),
     "lbm_reduce_workspace_bytes": ([_P, C.POINTER(C.c_size_t)], C.c_int),
     "lbm_mass_momentum": ([_P, _P, _P, _P, _P, C.c_size_t], C.c_int),
 }
@@ -145,6 +151,12 @@ class Plan:
 
     def reduce_workspace_bytes(self) -> int:
         return self._size(lib().lbm_reduce_workspace_bytes)
+
+    def adjoint_workspace_bytes(self, n_steps: int, checkpoint_every: int = 0) -> int:
+        n = C.c_size_t()
+        check(lib().lbm_adjoint_workspace_bytes(self._h, int(n_steps), int(checkpoint_every),
+                                                C.byref(n)))
+        return int(n.value)
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "../../include/lbm_b200.h"
+#include "lbm_adjoint.cuh"
 #include "lbm_kernels.cuh"
 
 struct lbm_plan {
@@ -177,6 +178,12 @@ int launch_step(const lbm::StepArgs& a, bool final_aos, cudaStream_t s) {
   return cuda_check(cudaGetLastError(), "k_step launch");
 }
 
+template <int Q, class S>
+int launch_step_moments_only(const lbm::StepArgs& a, cudaStream_t s) {
+  launch_step_mode<Q, S, lbm::kOutMoments>(a, s);
+  return cuda_check(cudaGetLastError(), "k_step launch");
+}
+
 // Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies.
 template <int Q, class S>
 int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
@@ -236,6 +243,196 @@ int do_steps(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* f_o
 }
 
 constexpr int kReduceBlocks = 148 * 4;
+
+// ---------------------------------------------------------------------------
+// Differentiated rollout: checkpointed forward + reverse sweep
+// ---------------------------------------------------------------------------
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+struct AdjLayout {
+  int64_t T = 0, K = 0, S = 0;  // steps, checkpoint interval, segments
+  size_t sb = 0;                // bytes of one population copy
+  size_t rho_bytes = 0, slot = 0;
+  size_t A = 0, B = 0, ck = 0, hist = 0, mu0 = 0, mu1 = 0, dF = 0, part = 0, total = 0;
+};
+
+int adj_layout(const lbm_plan* p, int64_t T, int64_t K, AdjLayout* L) {
+  if (T < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)T);
+  if (K <= 0) {
+    K = 1;
+    while (K * K < T) ++K;  // ceil(sqrt(T))
+  }
+  L->T = T;
+  L->K = K;
+  L->S = (T + K - 1) / K;
+  L->sb = align256(state_bytes(p));
+  L->rho_bytes = align256(static_cast<size_t>(p->g.ncell) * p->io);
+  L->slot = L->rho_bytes + align256(static_cast<size_t>(p->g.ncell) * p->D * p->io);
+  size_t o = 0;
+  L->A = o; o += L->sb;
+  L->B = o; o += L->sb;
+  L->ck = o; o += static_cast<size_t>(L->S - 1) * L->sb;
+  L->hist = o; o += static_cast<size_t>(K + 1) * L->slot;
+  L->mu0 = o; o += L->sb;
+  L->mu1 = o; o += L->sb;
+  L->dF = o; o += align256(static_cast<size_t>(p->g.ncell) * p->D * sizeof(double));
+  L->part = o; o += align256(sizeof(double) * 4 * kReduceBlocks);
+  L->total = o;
+  return LBM_OK;
+}
+
+int adj_check(const lbm_plan* p, const lbm_step_args* args) {
+  if (p == nullptr || args == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  if (p->storage != LBM_STORE_F32 && p->storage != LBM_STORE_F64)
+    return fail(LBM_ERR_UNSUPPORTED, "the differentiated rollout needs FP32 or FP64 storage");
+  if (args->inlet.kind != LBM_BC_NONE || args->outlet.kind != LBM_BC_NONE)
+    return fail(LBM_ERR_UNSUPPORTED,
+                "the differentiated rollout supports walls and body forces, not face conditions");
+  return LBM_OK;
+}
+
+template <int Q, class S>
+int adj_forward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
+                const AdjLayout& L, char* ws) {
+  char* AB[2] = {ws + L.A, ws + L.B};
+  auto slot = [&](int64_t j) { return ws + L.ck + static_cast<size_t>(j - 1) * L.sb; };
+  // Producer of p^m writes into checkpoint j = (m+1)/K when m+1 is a segment start.
+  auto out_for = [&](int64_t m, char* cur) -> char* {
+    if ((m + 1) % L.K == 0 && m + 1 < L.T) return slot((m + 1) / L.K);
+    return cur == AB[0] ? AB[1] : AB[0];
+  };
+  lbm::StepArgs m = a;
+  m.rho = m.vel = m.prs = nullptr;
+  m.f_in = f_in;
+  char* cur = out_for(0, nullptr);
+  planes(p, cur, const_cast<const void**>(m.pout));
+  int rc = launch_prepare<Q, S>(m, s);
+  if (rc) return rc;
+  for (int64_t n = 1; n < L.T; ++n) {
+    char* nxt = out_for(n, cur);
+    planes(p, cur, m.pin);
+    planes(p, nxt, const_cast<const void**>(m.pout));
+    rc = launch_step<Q, S>(m, false, s);
+    if (rc) return rc;
+    cur = nxt;
+  }
+  planes(p, cur, a.pin);
+  a.f_out = f_out;
+  return launch_step<Q, S>(a, true, s);
+}
+
+template <int Q, class S>
+int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in,
+                 const void* g_rho, const void* g_vel, const void* g_f, double* grad_force,
+                 void* grad_f_in, const AdjLayout& L, char* ws) {
+  using IO = typename lbm::StoreT<S>::IO;
+  char* AB[2] = {ws + L.A, ws + L.B};
+  char* MU[2] = {ws + L.mu0, ws + L.mu1};
+  auto slot = [&](int64_t j) { return ws + L.ck + static_cast<size_t>(j - 1) * L.sb; };
+  auto hist_rho = [&](int64_t j) { return ws + L.hist + static_cast<size_t>(j) * L.slot; };
+  auto hist_vel = [&](int64_t j) { return hist_rho(j) + L.rho_bytes; };
+  double* dF = reinterpret_cast<double*>(ws + L.dF);
+  const unsigned grid = grid_for(p->g.ncell);
+
+  lbm::AdjArgs q{};
+  q.g = p->g;
+  q.omega = a.omega;
+  q.guo_c = a.guo_c;
+  q.force_mode = a.force_mode;
+  for (int d = 0; d < 3; ++d) q.force[d] = a.force[d];
+  q.force_field = a.force_field;
+  q.wall = a.wall;
+  q.dF = grad_force != nullptr ? dF : nullptr;
+  const bool force = a.force_mode != 0;
+
+  lbm::StepArgs m = a;  // recompute steps: moments into the history, raw velocity
+  m.prs = nullptr;
+  m.mflags = lbm::kMomRawVelocity;
+  m.f_in = f_in;
+  int mu = 0;  // MU[mu] holds mu^{n+1}
+  int rc = LBM_OK;
+  for (int64_t sg = L.S - 1; sg >= 0; --sg) {
+    const int64_t n0 = sg * L.K;
+    const int64_t n1 = n0 + L.K < L.T ? n0 + L.K : L.T;
+    // (rho^n, u^n) for n in [n0, n1): recompute from the segment's checkpoint
+    char* cur = AB[0];
+    m.rho = hist_rho(0);
+    m.vel = hist_vel(0);
+    planes(p, cur, const_cast<const void**>(m.pout));
+    if (sg == 0) {
+      rc = launch_prepare<Q, S>(m, s);
+    } else {
+      planes(p, slot(sg), m.pin);
+      rc = launch_step<Q, S>(m, false, s);
+    }
+    if (rc) return rc;
+    for (int64_t n = n0 + 1; n < n1; ++n) {
+      char* nxt = cur == AB[0] ? AB[1] : AB[0];
+      m.rho = hist_rho(n - n0);
+      m.vel = hist_vel(n - n0);
+      planes(p, cur, m.pin);
+      planes(p, nxt, const_cast<const void**>(m.pout));
+      rc = launch_step<Q, S>(m, false, s);
+      if (rc) return rc;
+      cur = nxt;
+    }
+    if (sg == L.S - 1) {
+      // moments of f^T, then lambda^T from the output gradients
+      m.rho = hist_rho(n1 - n0);
+      m.vel = hist_vel(n1 - n0);
+      planes(p, cur, m.pin);
+      rc = launch_step_moments_only<Q, S>(m, s);
+      if (rc) return rc;
+      q.rho = hist_rho(n1 - n0);
+      q.vel = hist_vel(n1 - n0);
+      q.g_rho = g_rho;
+      q.g_vel = g_vel;
+      q.g_f = g_f;
+      planes(p, MU[mu], const_cast<const void**>(q.mout));
+      lbm::k_adj_init<Q, S><<<grid, lbm::kBlock, 0, s>>>(q);
+      rc = cuda_check(cudaGetLastError(), "k_adj_init launch");
+      if (rc) return rc;
+    }
+    for (int64_t n = n1 - 1; n >= n0; --n) {
+      q.rho = hist_rho(n - n0);
+      q.vel = hist_vel(n - n0);
+      planes(p, MU[mu], q.min);
+      planes(p, MU[1 - mu], const_cast<const void**>(q.mout));
+      const bool aos = n == 0 && grad_f_in != nullptr;
+      q.grad_f0 = grad_f_in;
+      if (aos) {
+        if (force) lbm::k_adj_step<Q, S, true, lbm::kAdjOutAoS><<<grid, lbm::kBlock, 0, s>>>(q);
+        else lbm::k_adj_step<Q, S, false, lbm::kAdjOutAoS><<<grid, lbm::kBlock, 0, s>>>(q);
+      } else {
+        if (force) lbm::k_adj_step<Q, S, true, lbm::kAdjOutState><<<grid, lbm::kBlock, 0, s>>>(q);
+        else lbm::k_adj_step<Q, S, false, lbm::kAdjOutState><<<grid, lbm::kBlock, 0, s>>>(q);
+      }
+      rc = cuda_check(cudaGetLastError(), "k_adj_step launch");
+      if (rc) return rc;
+      mu = 1 - mu;
+    }
+  }
+  if (grad_force != nullptr) {
+    if (a.force_mode == LBM_FORCE_UNIFORM) {
+      double* part = reinterpret_cast<double*>(ws + L.part);
+      if (p->D == 3)
+        lbm::k_field_sum_part<3><<<kReduceBlocks, lbm::kReduceThreads, 0, s>>>(dF, p->g.ncell, part);
+      else
+        lbm::k_field_sum_part<2><<<kReduceBlocks, lbm::kReduceThreads, 0, s>>>(dF, p->g.ncell, part);
+      lbm::k_field_sum_final<<<1, lbm::kReduceThreads, 0, s>>>(part, kReduceBlocks, p->D,
+                                                              grad_force);
+      rc = cuda_check(cudaGetLastError(), "k_field_sum launch");
+    } else {
+      rc = cuda_check(cudaMemcpyAsync(grad_force, dF,
+                                      static_cast<size_t>(p->g.ncell) * p->D * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, s),
+                      "cudaMemcpyAsync");
+    }
+  }
+  (void)sizeof(IO);
+  return rc;
+}
 
 }  // namespace
 
@@ -407,6 +604,70 @@ int lbm_update_noalloc(const lbm_plan* plan, lbm_stream_t stream, const void* f_
   const int rc = noalloc_scratch(&ws);
   if (rc) return rc;
   return do_steps(plan, stream, f_in, f_out, 1, args, out, ws, LBM_NOALLOC_SCRATCH_BYTES, 1);
+}
+
+int lbm_adjoint_workspace_bytes(const lbm_plan* plan, int64_t n_steps, int64_t checkpoint_every,
+                                size_t* bytes) {
+  if (plan == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  AdjLayout L;
+  const int rc = adj_layout(plan, n_steps, checkpoint_every, &L);
+  if (rc) return rc;
+  *bytes = L.total;
+  return LBM_OK;
+}
+
+int lbm_rollout_forward(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* f_out,
+                        int64_t n_steps, int64_t checkpoint_every, const lbm_step_args* args,
+                        const lbm_moments* out, void* workspace, size_t workspace_bytes) {
+  int rc = adj_check(p, args);
+  if (rc) return rc;
+  if (f_in == nullptr || f_out == nullptr) return fail(LBM_ERR_INVALID, "f_in/f_out is NULL");
+  AdjLayout L;
+  rc = adj_layout(p, n_steps, checkpoint_every, &L);
+  if (rc) return rc;
+  if (workspace == nullptr || workspace_bytes < L.total)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", L.total,
+                workspace_bytes);
+  lbm::StepArgs a;
+  rc = build_args(p, args, out, &a);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  if (p->storage == LBM_STORE_F64)
+    return p->Q == 19 ? adj_forward<19, double>(p, s, a, f_in, f_out, L, ws)
+                      : adj_forward<9, double>(p, s, a, f_in, f_out, L, ws);
+  return p->Q == 19 ? adj_forward<19, float>(p, s, a, f_in, f_out, L, ws)
+                    : adj_forward<9, float>(p, s, a, f_in, f_out, L, ws);
+}
+
+int lbm_rollout_backward(const lbm_plan* p, lbm_stream_t stream, const void* f_in,
+                         int64_t n_steps, int64_t checkpoint_every, const lbm_step_args* args,
+                         const void* grad_density, const void* grad_velocity, const void* grad_f,
+                         double* grad_force, void* grad_f_in, void* workspace,
+                         size_t workspace_bytes) {
+  int rc = adj_check(p, args);
+  if (rc) return rc;
+  if (f_in == nullptr) return fail(LBM_ERR_INVALID, "f_in is NULL");
+  AdjLayout L;
+  rc = adj_layout(p, n_steps, checkpoint_every, &L);
+  if (rc) return rc;
+  if (workspace == nullptr || workspace_bytes < L.total)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", L.total,
+                workspace_bytes);
+  lbm::StepArgs a;
+  rc = build_args(p, args, nullptr, &a);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  if (p->storage == LBM_STORE_F64)
+    return p->Q == 19 ? adj_backward<19, double>(p, s, a, f_in, grad_density, grad_velocity,
+                                                 grad_f, grad_force, grad_f_in, L, ws)
+                      : adj_backward<9, double>(p, s, a, f_in, grad_density, grad_velocity,
+                                                grad_f, grad_force, grad_f_in, L, ws);
+  return p->Q == 19 ? adj_backward<19, float>(p, s, a, f_in, grad_density, grad_velocity, grad_f,
+                                              grad_force, grad_f_in, L, ws)
+                    : adj_backward<9, float>(p, s, a, f_in, grad_density, grad_velocity, grad_f,
+                                             grad_force, grad_f_in, L, ws);
 }
 
 int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes) {

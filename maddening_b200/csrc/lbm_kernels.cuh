@@ -124,6 +124,7 @@ struct StepArgs {
 };
 
 constexpr uint32_t kMomDensityDev = 1u;
+constexpr uint32_t kMomRawVelocity = 2u;  // velocity not zeroed in wall cells
 
 // Uniform force in internal axis order; device-resident values (traced
 // scalars, dev_values[6..8]) override the host ones.
@@ -370,7 +371,7 @@ constexpr int kMinBlocks = LBM_STEP_MINB;
 template <class S>
 constexpr int min_blocks() { return sizeof(typename StoreT<S>::R) == 8 ? kMinBlocks / 2 : kMinBlocks; }
 
-enum StepMode : int { kOutState = 0, kOutAoS = 1 };
+enum StepMode : int { kOutState = 0, kOutAoS = 1, kOutMoments = 2 };
 
 struct Cell {
   uint32_t c;      // linear cell index
@@ -390,12 +391,12 @@ __device__ __forceinline__ Cell locate(const Geo& g, uint32_t c) {
 }
 
 template <int Q, class IO>
-__device__ __forceinline__ void load_force(const StepArgs& a, uint32_t c,
+__device__ __forceinline__ void load_force(const void* force_field, uint32_t c,
                                            typename StoreT<IO>::R (&F)[3]) {
   using R = typename StoreT<IO>::R;
   constexpr int D = Lat<Q>::D;
   constexpr int sh = 3 - D;
-  const IO* p = static_cast<const IO*>(a.force_field) + static_cast<size_t>(c) * D;
+  const IO* p = static_cast<const IO*>(force_field) + static_cast<size_t>(c) * D;
   F[0] = 0;
 #pragma unroll
   for (int d = 0; d < D; ++d) F[d + sh] = static_cast<R>(__ldg(p + d));
@@ -415,7 +416,9 @@ __device__ __forceinline__ void store_moments(const StepArgs& a, uint32_t c,
   if (a.vel != nullptr) {
     IO* v = static_cast<IO*>(a.vel) + static_cast<size_t>(c) * D;
 #pragma unroll
-    for (int d = 0; d < D; ++d) v[d] = wall ? IO(0) : static_cast<IO>(m.u[d + sh]);
+    const bool zero = wall && !(a.mflags & kMomRawVelocity);
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] = zero ? IO(0) : static_cast<IO>(m.u[d + sh]);
   }
 }
 
@@ -445,10 +448,12 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_prepare(const StepA
   for (int q = 0; q < Q; ++q) d[q] = to_offset<Q, R>(static_cast<R>(__ldg(fi + q)), q);
   R F[3] = {0, 0, 0};
   if (FORCE) {
-    if (a.force_mode == 2) load_force<Q, IO>(a, c, F);
+    if (a.force_mode == 2) load_force<Q, IO>(a.force_field, c, F);
     else uniform_force<Q, R>(a, F);
   }
   const Mom<R> m = moments<Q, R>(d, F);
+  if (a.rho != nullptr || a.vel != nullptr || a.prs != nullptr)
+    store_moments<Q, IO>(a, c, m, a.wall != nullptr && a.wall[c] != 0);
   collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
   for (int q = 0; q < Q; ++q) static_cast<S*>(a.pout[q])[c] = from_r<S>(d[q]);
@@ -489,7 +494,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_step(const StepArgs
   const bool wall = a.wall != nullptr && __ldg(a.wall + cidx) != 0;
   R F[3] = {0, 0, 0};
   if (FORCE) {
-    if (a.force_mode == 2) load_force<Q, IO>(a, cidx, F);
+    if (a.force_mode == 2) load_force<Q, IO>(a.force_field, cidx, F);
     else uniform_force<Q, R>(a, F);
   }
 
@@ -527,7 +532,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_step(const StepArgs
     IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(cidx) * Q;
 #pragma unroll
     for (int q = 0; q < Q; ++q) fo[q] = static_cast<IO>(from_offset<Q, R>(d[q], q));
-  } else {
+  } else if constexpr (MODE == kOutState) {
     collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
     for (int q = 0; q < Q; ++q) static_cast<S*>(a.pout[q])[cidx] = from_r<S>(d[q]);

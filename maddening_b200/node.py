@@ -391,6 +391,42 @@ class LBMNode(SimulationNode):
                                                   description="Runtime wall mask override (True=wall)"),
         }
 
+    # -- differentiable rollout --------------------------------------------------
+    def rollout(self, state: dict, boundary_inputs: dict, n_steps: int, *,
+                checkpoint_every: int = 0) -> dict:
+        """``n_steps`` fused steps, differentiable with respect to ``state["f"]``
+        and ``boundary_inputs["body_force"]`` (field or (D,)) through the
+        hand-written adjoint (``lbm_rollout_forward`` / ``lbm_rollout_backward``).
+
+        Populations are checkpointed every ``checkpoint_every`` steps (0: the
+        ceiling of sqrt(n_steps)); the backward recomputes each segment.  Walls
+        and body forces only (no face conditions); FP32 or FP64 storage.
+        """
+        if int(n_steps) < 1:
+            raise ValueError("n_steps must be >= 1")
+        bi = dict(boundary_inputs or {})
+        for key in ("inlet_pressure", "outlet_pressure", "inlet_velocity"):
+            if key in bi:
+                raise ValueError(f"rollout(): face condition '{key}' is not differentiable here")
+        if self._outlet_condition != "pressure":
+            raise ValueError("rollout(): the zero-gradient outlet is not differentiable here")
+        dev = self._dev()
+        f0 = torch.as_tensor(state["f"], device=dev)
+        if f0.dtype != self._io_dtype:
+            f0 = f0.to(self._io_dtype)
+        force = bi.pop("body_force", None)
+        if force is not None and not isinstance(force, torch.Tensor):
+            force = torch.as_tensor(np.asarray(force, dtype=np.float32), device=dev)
+        if force is not None:
+            force = force.to(device=dev)
+        wall_state = {k: v for k, v in state.items() if k == "wall_mask"}
+        f, rho, vel, prs = _RolloutFn.apply(f0, force, self, wall_state, bi, int(n_steps),
+                                            int(checkpoint_every))
+        out = {"f": f, "density": rho, "velocity": vel, "pressure": prs}
+        if "wall_mask" in state:
+            out["wall_mask"] = state["wall_mask"]
+        return out
+
     # -- diagnostics -----------------------------------------------------------
     def mass_momentum(self, f) -> torch.Tensor:
         """FP64 (sum rho, sum rho u) of a state f, reduced on the device."""
@@ -402,3 +438,73 @@ class LBMNode(SimulationNode):
         _lib.check(_lib.lib().lbm_mass_momentum(self._plan.handle, stream, f.data_ptr(),
                                                 out.data_ptr(), ws.data_ptr(), ws.numel()))
         return out[: 1 + self._D]
+
+
+class _RolloutFn(torch.autograd.Function):
+    """Fused rollout whose backward is the checkpointed hand-written adjoint."""
+
+    @staticmethod
+    def forward(ctx, f0, force, node, wall_state, bi, n_steps, checkpoint_every):
+        dev = f0.device
+        plan = node.plan
+        D, grid = node._D, node._grid_shape
+        bi_full = dict(bi)
+        keep = []
+        if force is not None:
+            if force.ndim == 1 and tuple(force.shape) == (D,):
+                bi_full["body_force"] = force.detach().to(torch.float32).cpu().numpy()
+            else:
+                ff = node._as_field(force.detach(), grid + (D,), dev)
+                keep.append(ff)
+                bi_full["body_force"] = ff
+        args, k2 = node._step_args(wall_state, bi_full, dev)
+        keep.extend(k2)
+        f_in = f0.detach().contiguous()
+        f_out, rho, vel, prs, mom = node._outputs(dev)
+        ws = torch.empty(plan.adjoint_workspace_bytes(n_steps, checkpoint_every),
+                         dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_rollout_forward(
+            plan.handle, stream, f_in.data_ptr(), f_out.data_ptr(), n_steps, checkpoint_every,
+            C.byref(args), C.byref(mom), ws.data_ptr(), ws.numel()))
+        ctx.node, ctx.args, ctx.keep, ctx.ws = node, args, keep, ws
+        ctx.n_steps, ctx.K = n_steps, checkpoint_every
+        ctx.force_shape = None if force is None else tuple(force.shape)
+        ctx.force_dtype = None if force is None else force.dtype
+        ctx.save_for_backward(f_in)
+        return f_out, rho, vel, prs
+
+    @staticmethod
+    def backward(ctx, g_f, g_rho, g_vel, g_prs):
+        (f_in,) = ctx.saved_tensors
+        node = ctx.node
+        dev = f_in.device
+        io = node._io_dtype
+        if g_prs is not None:  # pressure = density * cs2
+            g_rho = g_prs * node._cs2 if g_rho is None else g_rho + g_prs * node._cs2
+
+        def ptr(t):
+            return None if t is None else t.to(io).contiguous().data_ptr()
+
+        g_rho_c = None if g_rho is None else g_rho.to(io).contiguous()
+        g_vel_c = None if g_vel is None else g_vel.to(io).contiguous()
+        g_f_c = None if g_f is None else g_f.to(io).contiguous()
+        want_force = ctx.force_shape is not None and ctx.needs_input_grad[1]
+        want_f0 = ctx.needs_input_grad[0]
+        gF = None
+        if want_force:
+            n = node._D if len(ctx.force_shape) == 1 else int(np.prod(ctx.force_shape))
+            gF = torch.empty(n, dtype=torch.float64, device=dev)
+        gf0 = torch.empty_like(f_in) if want_f0 else None
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_rollout_backward(
+            node.plan.handle, stream, f_in.data_ptr(), ctx.n_steps, ctx.K, C.byref(ctx.args),
+            None if g_rho_c is None else g_rho_c.data_ptr(),
+            None if g_vel_c is None else g_vel_c.data_ptr(),
+            None if g_f_c is None else g_f_c.data_ptr(),
+            None if gF is None else gF.data_ptr(),
+            None if gf0 is None else gf0.data_ptr(), ctx.ws.data_ptr(), ctx.ws.numel()))
+        grad_force = None
+        if gF is not None:
+            grad_force = gF.reshape(ctx.force_shape).to(ctx.force_dtype)
+        return gf0, grad_force, None, None, None, None, None
