@@ -178,6 +178,32 @@ int lbm_rollout_backward(const lbm_plan* plan, lbm_stream_t stream, const void* 
                          double* grad_force, void* grad_f_in, void* workspace,
                          size_t workspace_bytes);
 
+/* ---- Batched ensemble ------------------------------------------------------
+ * Many independent lattices (own shape, tau, walls, force, faces; one lattice
+ * type and storage form) advanced together: every step is ONE persistent
+ * launch over a tile list of all instances (the reference runs a batch as
+ * jax.vmap over lax.scan, graph_manager.py:2807-2881, which needs equal shapes).
+ * Instance i behaves exactly like lbm_rollout with plans[i] and args[i]. */
+typedef struct lbm_batch lbm_batch;
+
+typedef struct {
+  int32_t blocks_per_sm; /* persistent grid = blocks_per_sm x SMs; 0 = one block per tile */
+  int32_t tile_order;    /* 0: instance after instance; 1: round-robin across instances */
+  int32_t use_graph;     /* 1: record the step sequence as a CUDA graph and replay it */
+} lbm_batch_config;
+
+/* plans[0..n-1] must outlive the batch and share lattice and storage. */
+int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** batch);
+int lbm_batch_destroy(lbm_batch* batch);
+int lbm_batch_workspace_bytes(const lbm_batch* batch, size_t* bytes);
+
+/* n_steps reference steps of every instance.  f_in[i] / f_out[i] / args[i] /
+ * out[i] (out may be NULL) are instance i's; cfg may be NULL (defaults). */
+int lbm_batch_rollout(const lbm_batch* batch, lbm_stream_t stream, const void* const* f_in,
+                      void* const* f_out, int64_t n_steps, const lbm_step_args* args,
+                      const lbm_moments* out, const lbm_batch_config* cfg, void* workspace,
+                      size_t workspace_bytes);
+
 /* Scratch capacity of lbm_update_noalloc: one population copy of at most
  * 24 MiB.  D3Q19: up to 331,129 cells with FP32 storage (e.g. 64^3), 662,258
  * with FP16/BF16, 165,564 with FP64; D2Q9: up to 699,050 cells with FP32. */

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/lbm_b200.h"
 #include "lbm_adjoint.cuh"
@@ -434,7 +435,56 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
   return rc;
 }
 
+// ---------------------------------------------------------------------------
+// Batched ensemble (host side)
+// ---------------------------------------------------------------------------
+
+template <int Q, class S>
+int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t ntiles, int64_t n,
+                unsigned grid, cudaStream_t s, cudaStream_t side, bool use_graph) {
+  lbm::k_batched_prepare<Q, S><<<grid, lbm::kBlock, 0, s>>>(args, tiles, ntiles);
+  int rc = cuda_check(cudaGetLastError(), "k_batched_prepare launch");
+  if (rc) return rc;
+  cudaStream_t ls = s;
+  cudaGraph_t graph = nullptr;
+  if (use_graph) {
+    // The step sequence is recorded on the batch's own stream (capture only
+    // records, nothing runs there) and replayed on the caller's stream, after
+    // the work already queued on it.
+    rc = cuda_check(cudaStreamBeginCapture(side, cudaStreamCaptureModeThreadLocal),
+                    "cudaStreamBeginCapture");
+    if (rc) return rc;
+    ls = side;
+  }
+  for (int64_t k = 1; k < n; ++k)
+    lbm::k_batched_step<Q, S, lbm::kOutState><<<grid, lbm::kBlock, 0, ls>>>(
+        args, tiles, ntiles, static_cast<int>(k % 2));
+  lbm::k_batched_step<Q, S, lbm::kOutAoS><<<grid, lbm::kBlock, 0, ls>>>(args, tiles, ntiles, 2);
+  rc = cuda_check(cudaGetLastError(), "k_batched_step launch");
+  if (use_graph) {
+    const int rc2 = cuda_check(cudaStreamEndCapture(side, &graph), "cudaStreamEndCapture");
+    if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+    if (rc2) return rc2;
+    cudaGraphExec_t exec = nullptr;
+    rc = cuda_check(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(graph);
+    if (rc) return rc;
+    rc = cuda_check(cudaGraphLaunch(exec, s), "cudaGraphLaunch");
+    cudaGraphExecDestroy(exec);  // released once the launched graph completes
+  }
+  return rc;
+}
+
 }  // namespace
+
+struct lbm_batch {
+  int n = 0, Q = 0, D = 0, storage = 0;
+  std::vector<const lbm_plan*> plans;
+  std::vector<size_t> state_off;  // instance i: two population copies at this offset
+  size_t args_off = 0, tiles_off[2] = {0, 0}, total = 0;
+  std::vector<lbm::BatchTile> tiles[2];  // [0] instance-major, [1] round-robin
+  cudaStream_t side = nullptr;
+};
 
 // Scratch of lbm_update_noalloc: one population copy, in the module's static
 // device memory (every GPU that loads the library holds it until exit).  In
@@ -668,6 +718,145 @@ int lbm_rollout_backward(const lbm_plan* p, lbm_stream_t stream, const void* f_i
                                               grad_force, grad_f_in, L, ws)
                     : adj_backward<9, float>(p, s, a, f_in, grad_density, grad_velocity, grad_f,
                                              grad_force, grad_f_in, L, ws);
+}
+
+int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
+  if (plans == nullptr || out == nullptr || n < 1) return fail(LBM_ERR_INVALID, "bad arguments");
+  *out = nullptr;
+  lbm_batch* b = new lbm_batch();
+  b->n = n;
+  b->Q = plans[0] ? plans[0]->Q : 0;
+  b->D = plans[0] ? plans[0]->D : 0;
+  b->storage = plans[0] ? plans[0]->storage : 0;
+  size_t o = 0;
+  b->args_off = o;
+  o += align256(sizeof(lbm::StepArgs) * lbm::kBatchArgs * static_cast<size_t>(n));
+  std::vector<std::vector<lbm::BatchTile>> per(n);
+  size_t ntiles = 0;
+  for (int i = 0; i < n; ++i) {
+    const lbm_plan* p = plans[i];
+    if (p == nullptr || p->Q != b->Q || p->storage != b->storage) {
+      delete b;
+      return fail(LBM_ERR_INVALID, "instance %d: plans must share lattice and storage", i);
+    }
+    b->plans.push_back(p);
+    for (uint32_t c = 0; c < p->g.ncell; c += lbm::kBlock)
+      per[i].push_back(lbm::BatchTile{static_cast<uint32_t>(i), c});
+    ntiles += per[i].size();
+  }
+  if (ntiles >= (size_t(1) << 31)) {
+    delete b;
+    return fail(LBM_ERR_INVALID, "ensemble too large");
+  }
+  for (int i = 0; i < n; ++i) b->tiles[0].insert(b->tiles[0].end(), per[i].begin(), per[i].end());
+  for (size_t r = 0;; ++r) {  // round-robin across instances
+    bool any = false;
+    for (int i = 0; i < n; ++i)
+      if (r < per[i].size()) { b->tiles[1].push_back(per[i][r]); any = true; }
+    if (!any) break;
+  }
+  for (int k = 0; k < 2; ++k) {
+    b->tiles_off[k] = o;
+    o += align256(sizeof(lbm::BatchTile) * ntiles);
+  }
+  for (int i = 0; i < n; ++i) {
+    b->state_off.push_back(o);
+    o += 2 * align256(state_bytes(plans[i]));
+  }
+  b->total = o;
+  if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess) b->side = nullptr;
+  *out = b;
+  return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch* b) {
+  if (b != nullptr && b->side != nullptr) cudaStreamDestroy(b->side);
+  delete b;
+  return LBM_OK;
+}
+
+int lbm_batch_workspace_bytes(const lbm_batch* b, size_t* bytes) {
+  if (b == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  *bytes = b->total;
+  return LBM_OK;
+}
+
+int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const* f_in,
+                      void* const* f_out, int64_t n_steps, const lbm_step_args* args,
+                      const lbm_moments* out, const lbm_batch_config* cfg, void* workspace,
+                      size_t workspace_bytes) {
+  if (b == nullptr || f_in == nullptr || f_out == nullptr || args == nullptr)
+    return fail(LBM_ERR_INVALID, "NULL argument");
+  if (n_steps < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)n_steps);
+  if (workspace == nullptr || workspace_bytes < b->total)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", b->total,
+                workspace_bytes);
+  lbm_batch_config c{0, 0, 0};
+  if (cfg != nullptr) c = *cfg;
+  if (c.tile_order < 0 || c.tile_order > 1 || c.blocks_per_sm < 0)
+    return fail(LBM_ERR_INVALID, "bad batch config");
+  if (c.use_graph && b->side == nullptr)
+    return fail(LBM_ERR_UNSUPPORTED, "no capture stream for CUDA-graph replay");
+  char* ws = static_cast<char*>(workspace);
+  std::vector<lbm::StepArgs> host(static_cast<size_t>(lbm::kBatchArgs) * b->n);
+  for (int i = 0; i < b->n; ++i) {
+    const lbm_plan* p = b->plans[i];
+    if (f_in[i] == nullptr || f_out[i] == nullptr)
+      return fail(LBM_ERR_INVALID, "instance %d: f_in/f_out is NULL", i);
+    lbm::StepArgs a;
+    int rc = build_args(p, &args[i], out != nullptr ? &out[i] : nullptr, &a);
+    if (rc) return rc;
+    char* A = ws + b->state_off[i];
+    char* B = A + align256(state_bytes(p));
+    lbm::StepArgs m = a;
+    m.rho = m.vel = m.prs = nullptr;
+    m.f_in = f_in[i];
+    lbm::StepArgs* h = &host[static_cast<size_t>(lbm::kBatchArgs) * i];
+    h[0] = m;
+    planes(p, B, h[0].pin);
+    planes(p, A, const_cast<const void**>(h[0].pout));
+    h[1] = m;
+    planes(p, A, h[1].pin);
+    planes(p, B, const_cast<const void**>(h[1].pout));
+    h[2] = a;  // last step: p^{n-1} is in A when n is odd, else in B
+    planes(p, n_steps % 2 == 1 ? A : B, h[2].pin);
+    h[2].f_out = f_out[i];
+  }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  lbm::StepArgs* dargs = reinterpret_cast<lbm::StepArgs*>(ws + b->args_off);
+  lbm::BatchTile* dtiles = reinterpret_cast<lbm::BatchTile*>(ws + b->tiles_off[c.tile_order]);
+  const auto& tl = b->tiles[c.tile_order];
+  int rc = cuda_check(cudaMemcpyAsync(dargs, host.data(), host.size() * sizeof(lbm::StepArgs),
+                                      cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+  if (rc) return rc;
+  rc = cuda_check(cudaMemcpyAsync(dtiles, tl.data(), tl.size() * sizeof(lbm::BatchTile),
+                                  cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+  if (rc) return rc;
+  const uint32_t ntiles = static_cast<uint32_t>(tl.size());
+  unsigned grid = ntiles;
+  if (c.blocks_per_sm > 0) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    grid = static_cast<unsigned>(c.blocks_per_sm) * static_cast<unsigned>(sms);
+    if (grid > ntiles) grid = ntiles;
+  }
+  const bool g = c.use_graph != 0;
+  switch (b->storage) {
+    case LBM_STORE_F32:
+      return b->Q == 19 ? batched_run<19, float>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
+                        : batched_run<9, float>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
+    case LBM_STORE_F16:
+      return b->Q == 19 ? batched_run<19, __half>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
+                        : batched_run<9, __half>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
+    case LBM_STORE_BF16:
+      return b->Q == 19 ? batched_run<19, __nv_bfloat16>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
+                        : batched_run<9, __nv_bfloat16>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
+    case LBM_STORE_F64:
+      return b->Q == 19 ? batched_run<19, double>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
+                        : batched_run<9, double>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
+  }
+  return fail(LBM_ERR_INVALID, "bad storage");
 }
 
 int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes) {

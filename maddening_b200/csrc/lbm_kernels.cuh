@@ -437,11 +437,9 @@ __device__ __forceinline__ R from_offset(R d, int q) {
 // Collide from a reference-layout state f (*grid_shape, Q): p = C(f).
 // Cell-local; the first pass of every update / rollout.
 template <int Q, class S, bool FORCE>
-__global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_prepare(const StepArgs a) {
+__device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
-  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= a.g.ncell) return;
   const IO* fi = static_cast<const IO*>(a.f_in) + static_cast<size_t>(c) * Q;
   R d[Q];
 #pragma unroll
@@ -459,15 +457,21 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_prepare(const StepA
   for (int q = 0; q < Q; ++q) static_cast<S*>(a.pout[q])[c] = from_r<S>(d[q]);
 }
 
-// One fused step: pull p -> wall swap -> faces (= reference f_bc) -> moments
-// (reference outputs) -> collide (next p) or write f_bc (MODE kOutAoS).
+template <int Q, class S, bool FORCE>
+__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+    k_prepare(const __grid_constant__ StepArgs a) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c < a.g.ncell) prepare_cell<Q, S, FORCE>(a, c);
+}
+
+// One fused step of cell cidx: pull p -> wall swap -> faces (= reference
+// f_bc) -> moments (reference outputs) -> collide (next p), or write f_bc
+// (MODE kOutAoS), or moments only (MODE kOutMoments).
 template <int Q, class S, int MODE, bool FACES, bool FORCE>
-__global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_step(const StepArgs a) {
+__device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
   const Geo& g = a.g;
-  const uint32_t cidx = blockIdx.x * kBlock + threadIdx.x;
-  if (cidx >= g.ncell) return;
   const Cell x = locate(g, cidx);
 
   // Offsets of the source rows of the pull x - e_q (periodic on every axis).
@@ -536,6 +540,93 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_step(const StepArgs
     collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
     for (int q = 0; q < Q; ++q) static_cast<S*>(a.pout[q])[cidx] = from_r<S>(d[q]);
+  }
+}
+
+template <int Q, class S, int MODE, bool FACES, bool FORCE>
+__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+    k_step(const __grid_constant__ StepArgs a) {
+  const uint32_t cidx = blockIdx.x * kBlock + threadIdx.x;
+  if (cidx < a.g.ncell) step_cell<Q, S, MODE, FACES, FORCE>(a, cidx);
+}
+
+// ---------------------------------------------------------------------------
+// Batched ensemble: many lattices (own shape, tau, force, walls) in one launch
+// ---------------------------------------------------------------------------
+
+// A tile is kBlock consecutive cells of one instance.
+struct BatchTile {
+  uint32_t inst;
+  uint32_t first;
+};
+
+// Argument blocks per instance: [0] p in B -> out A (also the first collide),
+// [1] p in A -> out B, [2] the last step (reference f and moments out).
+constexpr int kBatchArgs = 3;
+
+// Copies instance arguments into shared memory (the whole block reads them).
+__device__ __forceinline__ void stage_args(StepArgs& dst, const StepArgs& src) {
+  static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied as 32-bit words");
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(&src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+  for (int w = threadIdx.x; w < static_cast<int>(sizeof(StepArgs) / 4); w += kBlock) d[w] = s[w];
+}
+
+// The face / force specialisation of a member is chosen per tile at run time,
+// so every member runs exactly the kernel body its own rollout would.
+template <int Q, class S, int MODE>
+__device__ __forceinline__ void step_cell_any(const StepArgs& a, uint32_t c) {
+  const bool faces = a.face[0].kind != kFaceNone || a.face[1].kind != kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (faces) {
+    if (force) step_cell<Q, S, MODE, true, true>(a, c);
+    else step_cell<Q, S, MODE, true, false>(a, c);
+  } else {
+    if (force) step_cell<Q, S, MODE, false, true>(a, c);
+    else step_cell<Q, S, MODE, false, false>(a, c);
+  }
+}
+
+// Persistent launch: each block walks the tile list with a grid stride; tile
+// t uses args[kBatchArgs * inst + which], staged in shared memory.
+template <int Q, class S, int MODE>
+__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+    k_batched_step(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
+                   uint32_t ntiles, int which) {
+  __shared__ StepArgs sa;
+  uint32_t cur = 0xffffffffu;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    if (tile.inst != cur) {
+      __syncthreads();
+      stage_args(sa, args[kBatchArgs * tile.inst + which]);
+      __syncthreads();
+      cur = tile.inst;
+    }
+    const uint32_t c = tile.first + threadIdx.x;
+    if (c < sa.g.ncell) step_cell_any<Q, S, MODE>(sa, c);
+  }
+}
+
+template <int Q, class S>
+__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+    k_batched_prepare(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
+                      uint32_t ntiles) {
+  __shared__ StepArgs sa;
+  uint32_t cur = 0xffffffffu;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    if (tile.inst != cur) {
+      __syncthreads();
+      stage_args(sa, args[kBatchArgs * tile.inst]);
+      __syncthreads();
+      cur = tile.inst;
+    }
+    const uint32_t c = tile.first + threadIdx.x;
+    if (c < sa.g.ncell) {
+      if (sa.force_mode != 0) prepare_cell<Q, S, true>(sa, c);
+      else prepare_cell<Q, S, false>(sa, c);
+    }
   }
 }
 

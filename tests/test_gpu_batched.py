@@ -1,0 +1,97 @@
+"""Batched uneven ensemble (``LBMEnsemble`` / ``lbm_batch_rollout``).
+
+Every member of a batched rollout must equal its own ``LBMNode.run`` (the
+same arithmetic, so bit for bit), for every launch configuration the
+autotuner may pick; one member is also checked against the FP64 oracle.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lbm_ref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(storage="f32", lattice="D3Q19"):
+    from maddening_b200 import LBMNode
+    rng = np.random.default_rng(21)
+    if lattice == "D3Q19":
+        shapes = [(9, 7, 13), (16, 16, 16), (5, 12, 33), (20, 8, 6), (3, 4, 130), (11, 10, 9)]
+    else:
+        shapes = [(17, 9), (40, 33), (6, 131), (25, 4), (12, 12)]
+    nodes, bis, states = [], [], []
+    for i, shape in enumerate(shapes):
+        tau = float(rng.uniform(0.55, 1.5))
+        wall = rng.random(shape) < 0.1
+        kw = {}
+        bi = {"body_force": rng.uniform(-1e-5, 1e-5, len(shape)).astype(np.float32)}
+        if i == 1:
+            kw = dict(inlet_face="x_min", outlet_face="x_max")
+            wall[0] = wall[-1] = False
+            bi["inlet_pressure"] = np.float32(1.0 / 3.0 + 1e-3)
+            bi["outlet_pressure"] = np.float32(1.0 / 3.0)
+        if i == 2:
+            kw = dict(outlet_condition="zero_gradient")
+            wall[0] = wall[-1] = False
+            bi = {"inlet_velocity": np.array([0.03] + [0.0] * (len(shape) - 1))}
+        if i == 3:
+            bi["body_force"] = rng.uniform(-1e-5, 1e-5, shape + (len(shape),)).astype(np.float32)
+        node = LBMNode(f"m{i}", 1.0, grid_shape=shape, viscosity=(tau - 0.5) / 3.0,
+                       lattice=lattice, wall_mask=wall, storage=storage, **kw)
+        st = node.initial_state()
+        lat = node.lattice
+        f0 = lat.w * (1 + 1e-3 * rng.standard_normal(shape + (lat.Q,)))
+        st["f"] = torch.as_tensor(f0, device="cuda").to(st["f"].dtype)
+        nodes.append(node)
+        bis.append(bi)
+        states.append(st)
+    return nodes, bis, states
+
+
+CONFIGS = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g}
+           for b, o, g in ((0, 0, 0), (8, 0, 1), (4, 1, 0), (16, 1, 1), (1, 0, 1))]
+
+
+@pytest.mark.parametrize("lattice", ["D3Q19", "D2Q9"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+def test_batched_members_equal_their_own_rollouts(lattice, storage):
+    from maddening_b200.batched import LBMEnsemble
+    nodes, bis, states = _members(storage, lattice)
+    steps = 7
+    ref = [n.run(s, b, steps) for n, s, b in zip(nodes, states, bis)]
+    ens = LBMEnsemble(nodes)
+    for cfg in CONFIGS:
+        out = ens.run(states, bis, steps, cfg)
+        for i, (o, r) in enumerate(zip(out, ref)):
+            for key in ("f", "density", "velocity", "pressure"):
+                assert torch.equal(o[key], r[key]), (cfg, i, key)
+
+
+def test_batched_member_matches_fp64_oracle():
+    from maddening_b200.batched import LBMEnsemble
+    nodes, bis, states = _members("f64")
+    ens = LBMEnsemble(nodes)
+    out = ens.run(states, bis, 5)
+    i = 0
+    node = nodes[i]
+    orc = R.OracleLBM(node._grid_shape, node.viscosity, "D3Q19", wall_mask=node._wall_np)
+    so = orc.initial_state()
+    so["f"] = states[i]["f"].cpu().numpy()
+    so = orc.run(so, bis[i], 5)
+    np.testing.assert_allclose(out[i]["f"].cpu().numpy(), so["f"], rtol=0, atol=1e-14)
+    np.testing.assert_allclose(out[i]["velocity"].cpu().numpy(), so["velocity"], rtol=0, atol=1e-14)
+
+
+def test_autotune_picks_a_valid_config():
+    from maddening_b200.batched import LBMEnsemble
+    nodes, bis, states = _members()
+    ens = LBMEnsemble(nodes)
+    cfg = ens.autotune(states, bis, n_steps=4, use_cache=False)
+    assert cfg in [{"blocks_per_sm": b, "tile_order": o, "use_graph": g}
+                   for b in (0, 4, 8, 16) for o in (0, 1) for g in (0, 1)]
+    ref = [n.run(s, b, 3) for n, s, b in zip(nodes, states, bis)]
+    out = ens.run(states, bis, 3)
+    for o, r in zip(out, ref):
+        assert torch.equal(o["f"], r["f"])
