@@ -80,11 +80,19 @@ typedef struct {
   double value[3];
 } lbm_face_bc;
 
+/* lbm_desc.flags */
+#define LBM_PLAN_STAGED_ROWS 1u /* rollout steps stage neighbour rows in shared
+                                   memory with bulk async copies (rows of >= 128
+                                   cells and a multiple of 16 bytes); slower than
+                                   the default global gather on B200, kept for
+                                   comparison */
+
 typedef struct {
   int32_t lattice;  /* lbm_lattice: 19 (D3Q19) or 9 (D2Q9)                */
   int32_t storage;  /* lbm_storage                                        */
   int64_t shape[3]; /* grid_shape; shape[2] is ignored for D2Q9           */
   double tau;       /* BGK relaxation time, tau = 0.5 + viscosity / cs2    */
+  uint32_t flags;   /* LBM_PLAN_* bits, 0 = defaults                       */
 } lbm_desc;
 
 /* Per-call inputs of one step (the reference's boundary_inputs). */

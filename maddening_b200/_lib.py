@@ -35,9 +35,12 @@ class LbmError(RuntimeError):
         self.status = status
 
 
+PLAN_STAGED_ROWS = 1
+
+
 class lbm_desc(C.Structure):
     _fields_ = [("lattice", C.c_int32), ("storage", C.c_int32),
-                ("shape", C.c_int64 * 3), ("tau", C.c_double)]
+                ("shape", C.c_int64 * 3), ("tau", C.c_double), ("flags", C.c_uint32)]
 
 
 class lbm_face_bc(C.Structure):
@@ -119,10 +122,11 @@ def check(status: int) -> None:
 class Plan:
     """Owns one ``lbm_plan`` (immutable lattice/shape/tau/storage)."""
 
-    def __init__(self, q: int, shape, tau: float, storage: str = "f32"):
+    def __init__(self, q: int, shape, tau: float, storage: str = "f32", flags: int = 0):
         d = lbm_desc()
         d.lattice = q
         d.storage = STORAGE[storage]
+        d.flags = int(flags)
         for i, n in enumerate(tuple(shape)[:3]):
             d.shape[i] = int(n)
         d.tau = float(tau)

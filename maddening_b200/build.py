@@ -19,7 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblbm_b200.so"
 SOURCES = ["lbm_abi.cu"]
-HEADERS = ["lbm_kernels.cuh", "lbm_lattice.cuh", "lbm_adjoint.cuh"]
+HEADERS = ["lbm_kernels.cuh", "lbm_lattice.cuh", "lbm_adjoint.cuh", "lbm_staged.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",

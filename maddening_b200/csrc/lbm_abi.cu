@@ -13,6 +13,7 @@
 #include "../../include/lbm_b200.h"
 #include "lbm_adjoint.cuh"
 #include "lbm_kernels.cuh"
+#include "lbm_staged.cuh"
 
 struct lbm_plan {
   int Q = 0, D = 0, storage = 0;
@@ -21,6 +22,7 @@ struct lbm_plan {
   double tau = 0;
   size_t elem = 4;               // bytes per stored population
   size_t io = 4;                 // bytes per f / force / moment element
+  uint32_t flags = 0;            // LBM_PLAN_* bits
 };
 
 namespace {
@@ -41,6 +43,8 @@ int cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   return LBM_OK;
 }
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
 size_t state_bytes(const lbm_plan* p) {
   return static_cast<size_t>(p->Q) * static_cast<size_t>(p->g.ncell) * p->elem;
@@ -70,12 +74,7 @@ bool fastdiv_ok(const lbm::FastDiv& f, uint32_t xmax) {
   return true;
 }
 
-// Population plane pointers of a state buffer.
-void planes(const lbm_plan* p, const void* base, const void** out) {
-  const char* b = static_cast<const char*>(base);
-  for (int q = 0; q < p->Q; ++q)
-    out[q] = b + static_cast<size_t>(q) * p->g.ncell * p->elem;
-}
+
 
 // Maps one face condition of the ABI to the kernel form (internal axes).
 int map_face(const lbm_plan* p, const lbm_face_bc& in, bool is_outlet, lbm::FaceK* out) {
@@ -179,35 +178,95 @@ int launch_step(const lbm::StepArgs& a, bool final_aos, cudaStream_t s) {
   return cuda_check(cudaGetLastError(), "k_step launch");
 }
 
+// Row-staged state step (lbm_staged.cuh, opt-in LBM_PLAN_STAGED_ROWS): shape
+// and shared memory per storage; rows shorter than 128 cells keep the gather.
+template <class S>
+constexpr int staged_stages() { return sizeof(S) == 2 ? 3 : 2; }
+
+template <int Q, class S>
+bool staged_ok(const lbm_plan* p) {
+  const size_t row = static_cast<size_t>(p->g.n2) * sizeof(S);
+  const size_t smem = staged_stages<S>() * static_cast<size_t>(Q) * row + 64;
+  return (p->flags & LBM_PLAN_STAGED_ROWS) != 0 && row % 16 == 0 && p->g.n2 >= 128 &&
+         smem <= 200 * 1024;
+}
+
+template <int Q, class S, bool FACES, bool FORCE, int T>
+int launch_staged_t(const lbm::StepArgs& a, cudaStream_t s) {
+  auto kern = lbm::k_step_staged<Q, S, FACES, FORCE, T>;
+  const int stages = staged_stages<S>();
+  const size_t smem = static_cast<size_t>(stages) * Q * a.g.n2 * sizeof(S) + 64;
+  int rc = cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(smem)),
+                      "cudaFuncSetAttribute");
+  if (rc) return rc;
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem),
+                  "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+  if (rc) return rc;
+  if (per_sm < 1) per_sm = 1;
+  const uint32_t nrows = a.g.n0 * a.g.n1;
+  uint32_t grid = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(sms);
+  if (grid > nrows) grid = nrows;
+  kern<<<grid, T, smem, s>>>(a, stages);
+  return cuda_check(cudaGetLastError(), "k_step_staged launch");
+}
+
+template <int Q, class S>
+int launch_staged(const lbm::StepArgs& a, cudaStream_t s) {
+  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (a.g.n2 >= 256) {
+    if (faces) return force ? launch_staged_t<Q, S, true, true, 256>(a, s)
+                            : launch_staged_t<Q, S, true, false, 256>(a, s);
+    return force ? launch_staged_t<Q, S, false, true, 256>(a, s)
+                 : launch_staged_t<Q, S, false, false, 256>(a, s);
+  }
+  if (faces) return force ? launch_staged_t<Q, S, true, true, 128>(a, s)
+                          : launch_staged_t<Q, S, true, false, 128>(a, s);
+  return force ? launch_staged_t<Q, S, false, true, 128>(a, s)
+               : launch_staged_t<Q, S, false, false, 128>(a, s);
+}
+
 template <int Q, class S>
 int launch_step_moments_only(const lbm::StepArgs& a, cudaStream_t s) {
   launch_step_mode<Q, S, lbm::kOutMoments>(a, s);
   return cuda_check(cudaGetLastError(), "k_step launch");
 }
 
-// Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies.
+// Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies
+// (with n > 1 also the status word after them).
 template <int Q, class S>
 int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
               int64_t n, char* ws) {
-  const size_t sb = state_bytes(p);
+  const size_t sb = align256(state_bytes(p));
   char* A = ws;
   char* B = ws + sb;
   a.f_in = f_in;
-  planes(p, A, const_cast<const void**>(a.pout));
+  a.pout = A;
   int rc = launch_prepare<Q, S>(a, s);
   if (rc) return rc;
   lbm::StepArgs m = a;  // intermediate steps write no moments
   m.rho = m.vel = m.prs = nullptr;
+  // The bulk copies need 16-byte aligned rows: the caller's workspace too.
+  const bool staged = n > 1 && staged_ok<Q, S>(p) && reinterpret_cast<uintptr_t>(ws) % 16 == 0;
+  if (staged) {
+    m.status = reinterpret_cast<int*>(ws + 2 * sb);
+    rc = cuda_check(cudaMemsetAsync(m.status, 0, sizeof(int), s), "cudaMemsetAsync");
+    if (rc) return rc;
+  }
   for (int64_t i = 0; i + 1 < n; ++i) {
-    planes(p, A, m.pin);
-    planes(p, B, const_cast<const void**>(m.pout));
-    rc = launch_step<Q, S>(m, false, s);
+    m.pin = A;
+    m.pout = B;
+    rc = staged ? launch_staged<Q, S>(m, s) : launch_step<Q, S>(m, false, s);
     if (rc) return rc;
     char* t = A;
     A = B;
     B = t;
   }
-  planes(p, A, a.pin);
+  a.pin = A;
   a.f_out = f_out;
   return launch_step<Q, S>(a, true, s);
 }
@@ -230,7 +289,7 @@ int do_steps(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* f_o
   if (p == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
   if (f_in == nullptr || f_out == nullptr) return fail(LBM_ERR_INVALID, "f_in/f_out is NULL");
   if (n < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)n);
-  const size_t need = static_cast<size_t>(nbuf) * state_bytes(p);
+  const size_t need = nbuf == 1 ? state_bytes(p) : 2 * align256(state_bytes(p)) + 256;
   if (workspace == nullptr || workspace_bytes < need)
     return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", need,
                 workspace_bytes);
@@ -248,8 +307,6 @@ constexpr int kReduceBlocks = 148 * 4;
 // ---------------------------------------------------------------------------
 // Differentiated rollout: checkpointed forward + reverse sweep
 // ---------------------------------------------------------------------------
-
-size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
 struct AdjLayout {
   int64_t T = 0, K = 0, S = 0;  // steps, checkpoint interval, segments
@@ -307,18 +364,18 @@ int adj_forward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* 
   m.rho = m.vel = m.prs = nullptr;
   m.f_in = f_in;
   char* cur = out_for(0, nullptr);
-  planes(p, cur, const_cast<const void**>(m.pout));
+  m.pout = cur;
   int rc = launch_prepare<Q, S>(m, s);
   if (rc) return rc;
   for (int64_t n = 1; n < L.T; ++n) {
     char* nxt = out_for(n, cur);
-    planes(p, cur, m.pin);
-    planes(p, nxt, const_cast<const void**>(m.pout));
+    m.pin = cur;
+    m.pout = nxt;
     rc = launch_step<Q, S>(m, false, s);
     if (rc) return rc;
     cur = nxt;
   }
-  planes(p, cur, a.pin);
+  a.pin = cur;
   a.f_out = f_out;
   return launch_step<Q, S>(a, true, s);
 }
@@ -360,11 +417,11 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
     char* cur = AB[0];
     m.rho = hist_rho(0);
     m.vel = hist_vel(0);
-    planes(p, cur, const_cast<const void**>(m.pout));
+    m.pout = cur;
     if (sg == 0) {
       rc = launch_prepare<Q, S>(m, s);
     } else {
-      planes(p, slot(sg), m.pin);
+      m.pin = slot(sg);
       rc = launch_step<Q, S>(m, false, s);
     }
     if (rc) return rc;
@@ -372,8 +429,8 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
       char* nxt = cur == AB[0] ? AB[1] : AB[0];
       m.rho = hist_rho(n - n0);
       m.vel = hist_vel(n - n0);
-      planes(p, cur, m.pin);
-      planes(p, nxt, const_cast<const void**>(m.pout));
+      m.pin = cur;
+      m.pout = nxt;
       rc = launch_step<Q, S>(m, false, s);
       if (rc) return rc;
       cur = nxt;
@@ -382,7 +439,7 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
       // moments of f^T, then lambda^T from the output gradients
       m.rho = hist_rho(n1 - n0);
       m.vel = hist_vel(n1 - n0);
-      planes(p, cur, m.pin);
+      m.pin = cur;
       rc = launch_step_moments_only<Q, S>(m, s);
       if (rc) return rc;
       q.rho = hist_rho(n1 - n0);
@@ -390,7 +447,7 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
       q.g_rho = g_rho;
       q.g_vel = g_vel;
       q.g_f = g_f;
-      planes(p, MU[mu], const_cast<const void**>(q.mout));
+      q.mout = MU[mu];
       lbm::k_adj_init<Q, S><<<grid, lbm::kBlock, 0, s>>>(q);
       rc = cuda_check(cudaGetLastError(), "k_adj_init launch");
       if (rc) return rc;
@@ -398,8 +455,8 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
     for (int64_t n = n1 - 1; n >= n0; --n) {
       q.rho = hist_rho(n - n0);
       q.vel = hist_vel(n - n0);
-      planes(p, MU[mu], q.min);
-      planes(p, MU[1 - mu], const_cast<const void**>(q.mout));
+      q.min = MU[mu];
+      q.mout = MU[1 - mu];
       const bool aos = n == 0 && grad_f_in != nullptr;
       q.grad_f0 = grad_f_in;
       if (aos) {
@@ -543,6 +600,7 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
   p->D = desc->lattice == LBM_D3Q19 ? 3 : 2;
   p->storage = desc->storage;
   p->tau = desc->tau;
+  p->flags = desc->flags;
   int64_t dims[3];
   for (int d = 0; d < p->D; ++d) {
     if (desc->shape[d] < 1 || desc->shape[d] > (1 << 20)) {
@@ -558,9 +616,11 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
     dims[0] = 1; dims[1] = p->shape[0]; dims[2] = p->shape[1];
   }
   const int64_t ncell = dims[0] * dims[1] * dims[2];
-  if (ncell >= (int64_t(1) << 31)) {
+  if (ncell * p->Q >= (int64_t(1) << 32)) {
     delete p;
-    return fail(LBM_ERR_INVALID, "lattice of %lld cells is too large", (long long)ncell);
+    return fail(LBM_ERR_INVALID,
+                "lattice of %lld cells is too large: Q x cells must stay below 2^32",
+                (long long)ncell);
   }
   switch (p->storage) {
     case LBM_STORE_F32: p->elem = 4; p->io = 4; break;
@@ -597,7 +657,7 @@ int lbm_state_bytes(const lbm_plan* plan, size_t* bytes) {
 
 int lbm_workspace_bytes(const lbm_plan* plan, size_t* bytes) {
   if (plan == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
-  *bytes = 2 * state_bytes(plan);
+  *bytes = 2 * align256(state_bytes(plan)) + 256;
   return LBM_OK;
 }
 
@@ -813,13 +873,13 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
     m.f_in = f_in[i];
     lbm::StepArgs* h = &host[static_cast<size_t>(lbm::kBatchArgs) * i];
     h[0] = m;
-    planes(p, B, h[0].pin);
-    planes(p, A, const_cast<const void**>(h[0].pout));
+    h[0].pin = B;
+    h[0].pout = A;
     h[1] = m;
-    planes(p, A, h[1].pin);
-    planes(p, B, const_cast<const void**>(h[1].pout));
+    h[1].pin = A;
+    h[1].pout = B;
     h[2] = a;  // last step: p^{n-1} is in A when n is odd, else in B
-    planes(p, n_steps % 2 == 1 ? A : B, h[2].pin);
+    h[2].pin = n_steps % 2 == 1 ? A : B;
     h[2].f_out = f_out[i];
   }
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

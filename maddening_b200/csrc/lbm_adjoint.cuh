@@ -32,8 +32,8 @@ struct AdjArgs {
   double force[3];  // internal axis order
   const void* force_field;
   const uint8_t* wall;
-  const void* min[kMaxQ];  // mu^{n+1} planes (S)
-  void* mout[kMaxQ];       // mu^n planes (S)
+  const void* min;  // mu^{n+1} (S), direction q of cell c at [q * ncell + c]
+  void* mout;       // mu^n (S)
   const void* rho;         // rho^n  (IO, grid)
   const void* vel;         // u^n    (IO, (grid, D), not zeroed in walls)
   double* dF;              // dL/dF accumulator ((grid, D), reference order) or null
@@ -59,7 +59,8 @@ __device__ __forceinline__ void adj_store(const AdjArgs& a, uint32_t c,
     }
   }
 #pragma unroll
-  for (int q = 0; q < Q; ++q) static_cast<S*>(a.mout[q])[c] = from_r<S>(lam[q]);
+  for (int q = 0; q < Q; ++q)
+    static_cast<S*>(a.mout)[static_cast<uint32_t>(q) * a.g.ncell + c] = from_r<S>(lam[q]);
 }
 
 // lambda^T from the gradients of the step-T outputs (density, velocity with
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>()) k_adj_step(const AdjA
     if (c1 > 0) off += dp1;
     if (c1 < 0) off += dm1;
     off += c2 > 0 ? kp : (c2 < 0 ? km : x.k);
-    nu[q] = ld_pop<S>(static_cast<const S*>(a.min[q]) + off);
+    nu[q] = ld_pop<S>(static_cast<const S*>(a.min) + (static_cast<uint32_t>(q) * g.ncell + off));
   }
 
   const bool wall = a.wall != nullptr && __ldg(a.wall + cidx) != 0;

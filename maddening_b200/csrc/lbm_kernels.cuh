@@ -113,14 +113,18 @@ struct StepArgs {
   const uint8_t* wall;
   FaceK face[2];  // [0] inlet, [1] outlet
   const float* dev_values;
-  const void* pin[kMaxQ];  // state planes in  (S), one pointer per population
-  void* pout[kMaxQ];       // state planes out (S)
+  // State buffers (S): population q of cell c at base[q * ncell + c].  The
+  // index is 32-bit (plans keep Q x ncell < 2^32): one wide multiply-add per
+  // access forms the address.
+  const void* pin;
+  void* pout;
   const void* f_in;        // AoS IO (prepare)
   void* f_out;             // AoS IO (final step)
   void* rho;
   void* vel;
   void* prs;
   uint32_t mflags;
+  int* status;  // device word; bit 0 set when a bounded wait gave up (staged path)
 };
 
 constexpr uint32_t kMomDensityDev = 1u;
@@ -328,11 +332,8 @@ __device__ __forceinline__ typename StoreT<S>::R fbc_at(const StepArgs& a, int q
   const uint32_t j0 = wrapu(i0 + s * Lat<Q>::c0(q), g.n0);
   const uint32_t j1 = wrapu(i1 + s * Lat<Q>::c1(q), g.n1);
   const uint32_t j2 = wrapu(k + s * Lat<Q>::c2(q), g.n2);
-  const S* plane = nullptr;
-#pragma unroll
-  for (int t = 0; t < Q; ++t)
-    if (t == qs) plane = static_cast<const S*>(a.pin[t]);
-  return ld_pop<S>(plane + (j0 * g.n1 + j1) * g.n2 + j2);
+  return ld_pop<S>(static_cast<const S*>(a.pin) +
+                   (static_cast<uint32_t>(qs) * g.ncell + (j0 * g.n1 + j1) * g.n2 + j2));
 }
 
 // Zero-gradient face (extension): unknown q <- f_bc of the neighbour one
@@ -415,7 +416,6 @@ __device__ __forceinline__ void store_moments(const StepArgs& a, uint32_t c,
   }
   if (a.vel != nullptr) {
     IO* v = static_cast<IO*>(a.vel) + static_cast<size_t>(c) * D;
-#pragma unroll
     const bool zero = wall && !(a.mflags & kMomRawVelocity);
 #pragma unroll
     for (int d = 0; d < D; ++d) v[d] = zero ? IO(0) : static_cast<IO>(m.u[d + sh]);
@@ -454,7 +454,8 @@ __device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
     store_moments<Q, IO>(a, c, m, a.wall != nullptr && a.wall[c] != 0);
   collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
-  for (int q = 0; q < Q; ++q) static_cast<S*>(a.pout[q])[c] = from_r<S>(d[q]);
+  for (int q = 0; q < Q; ++q)
+    static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * a.g.ncell + c] = from_r<S>(d[q]);
 }
 
 template <int Q, class S, bool FORCE>
@@ -464,37 +465,17 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
   if (c < a.g.ncell) prepare_cell<Q, S, FORCE>(a, c);
 }
 
-// One fused step of cell cidx: pull p -> wall swap -> faces (= reference
-// f_bc) -> moments (reference outputs) -> collide (next p), or write f_bc
-// (MODE kOutAoS), or moments only (MODE kOutMoments).
+// Everything of one fused step after the pull (d = the pulled populations of
+// cell x): wall swap -> faces (= reference f_bc) -> moments (reference
+// outputs) -> collide (next p), or write f_bc (MODE kOutAoS), or moments only
+// (MODE kOutMoments).
 template <int Q, class S, int MODE, bool FACES, bool FORCE>
-__device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
+__device__ __forceinline__ void finish_cell(const StepArgs& a, const Cell& x,
+                                            typename StoreT<S>::R (&d)[Q]) {
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
   const Geo& g = a.g;
-  const Cell x = locate(g, cidx);
-
-  // Offsets of the source rows of the pull x - e_q (periodic on every axis).
-  const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
-  const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
-  const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.n2 : 0u - g.n2;  // i1 - 1
-  const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.n2 : g.n2;
-  const uint32_t km = x.k == 0 ? g.n2 - 1 : x.k - 1;
-  const uint32_t kp = x.k == g.n2 - 1 ? 0 : x.k + 1;
-
-  R d[Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
-    uint32_t off = x.row;
-    if (c0 > 0) off += dm0;
-    if (c0 < 0) off += dp0;
-    if (c1 > 0) off += dm1;
-    if (c1 < 0) off += dp1;
-    off += c2 > 0 ? km : (c2 < 0 ? kp : x.k);
-    d[q] = ld_pop<S>(static_cast<const S*>(a.pin[q]) + off);
-  }
-
+  const uint32_t cidx = x.c;
   const bool wall = a.wall != nullptr && __ldg(a.wall + cidx) != 0;
   R F[3] = {0, 0, 0};
   if (FORCE) {
@@ -539,8 +520,39 @@ __device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
   } else if constexpr (MODE == kOutState) {
     collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
-    for (int q = 0; q < Q; ++q) static_cast<S*>(a.pout[q])[cidx] = from_r<S>(d[q]);
+    for (int q = 0; q < Q; ++q)
+      static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * g.ncell + cidx] = from_r<S>(d[q]);
   }
+}
+
+// One fused step of cell cidx: pull p from global memory, then finish_cell.
+template <int Q, class S, int MODE, bool FACES, bool FORCE>
+__device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
+  using R = typename StoreT<S>::R;
+  const Geo& g = a.g;
+  const Cell x = locate(g, cidx);
+
+  // Offsets of the source rows of the pull x - e_q (periodic on every axis).
+  const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
+  const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
+  const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.n2 : 0u - g.n2;  // i1 - 1
+  const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.n2 : g.n2;
+  const uint32_t km = x.k == 0 ? g.n2 - 1 : x.k - 1;
+  const uint32_t kp = x.k == g.n2 - 1 ? 0 : x.k + 1;
+
+  R d[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
+    uint32_t off = x.row;
+    if (c0 > 0) off += dm0;
+    if (c0 < 0) off += dp0;
+    if (c1 > 0) off += dm1;
+    if (c1 < 0) off += dp1;
+    off += c2 > 0 ? km : (c2 < 0 ? kp : x.k);
+    d[q] = ld_pop<S>(static_cast<const S*>(a.pin) + (static_cast<uint32_t>(q) * g.ncell + off));
+  }
+  finish_cell<Q, S, MODE, FACES, FORCE>(a, x, d);
 }
 
 template <int Q, class S, int MODE, bool FACES, bool FORCE>

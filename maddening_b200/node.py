@@ -85,7 +85,7 @@ class LBMNode(SimulationNode):
                  wall_mask: Optional[np.ndarray] = None, inlet_face: str = "x_min",
                  outlet_face: str = "x_max", geometry_source: Optional[str] = None,
                  *, outlet_condition: str = "pressure", storage: str = "f32",
-                 device=None):
+                 device=None, staged_rows: bool = False):
         lat = by_name(lattice)
         if len(grid_shape) != lat.D:
             raise ValueError(f"grid_shape has {len(grid_shape)} dims but lattice "
@@ -131,7 +131,8 @@ class LBMNode(SimulationNode):
             self._wall_np = np.zeros(self._grid_shape, dtype=bool)
         self._has_walls = bool(self._wall_np.any())
         self._wall_dev = {}
-        self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage)
+        self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage,
+                               _lib.PLAN_STAGED_ROWS if staged_rows else 0)
 
     # -- properties (lbm.py:690-703) ---------------------------------------
     @property
@@ -326,8 +327,8 @@ class LBMNode(SimulationNode):
         f_in = self._f_in(state, dev)
         args, keep = self._step_args(state, boundary_inputs or {}, dev)
         f, rho, vel, prs, m = self._outputs(dev)
-        nbuf = 2 if n_steps > 1 else 1
-        ws = torch.empty(nbuf * self._plan.state_bytes(), dtype=torch.uint8, device=dev)
+        nbytes = self._plan.workspace_bytes() if n_steps > 1 else self._plan.state_bytes()
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
         lib = _lib.lib()
         if n_steps == 1:

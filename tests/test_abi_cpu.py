@@ -45,7 +45,8 @@ def test_struct_layout_matches_header():
              offsetof(lbm_step_args, force_field), offsetof(lbm_step_args, wall),
              offsetof(lbm_step_args, inlet), offsetof(lbm_step_args, outlet),
              offsetof(lbm_step_args, dev_values));
-      printf("%zu %zu\n", offsetof(lbm_desc, shape), offsetof(lbm_desc, tau));
+      printf("%zu %zu %zu\n", offsetof(lbm_desc, shape), offsetof(lbm_desc, tau),
+             offsetof(lbm_desc, flags));
       return 0;
     }
     """
@@ -63,7 +64,8 @@ def test_struct_layout_matches_header():
     assert offs == [S.force.offset, S.force_field.offset, S.wall.offset, S.inlet.offset,
                     S.outlet.offset, S.dev_values.offset]
     doffs = [int(x) for x in lines[2].split()]
-    assert doffs == [_lib.lbm_desc.shape.offset, _lib.lbm_desc.tau.offset]
+    assert doffs == [_lib.lbm_desc.shape.offset, _lib.lbm_desc.tau.offset,
+                     _lib.lbm_desc.flags.offset]
 
 
 @pytest.mark.parametrize("q,shape,tau,msg", [
@@ -82,7 +84,8 @@ def test_plan_sizes():
     p = _lib.Plan(19, (16, 12, 8), 0.8)
     n = 16 * 12 * 8
     assert p.state_bytes() == 19 * n * 4
-    assert p.workspace_bytes() == 2 * 19 * n * 4
+    sb = (19 * n * 4 + 255) // 256 * 256
+    assert p.workspace_bytes() == 2 * sb + 256  # two population copies + status word
     p16 = _lib.Plan(19, (16, 12, 8), 0.8, "f16")
     assert p16.state_bytes() == 19 * n * 2
     p64 = _lib.Plan(9, (16, 12), 0.8, "f64")
