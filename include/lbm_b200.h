@@ -86,6 +86,12 @@ typedef struct {
                                    cells and a multiple of 16 bytes); slower than
                                    the default global gather on B200, kept for
                                    comparison */
+#define LBM_PLAN_SINGLE_CELLS 2u /* rollout steps update one cell per thread
+                                   (the paired two-cell step is otherwise used
+                                   for FP16/BF16 storage when the contiguous
+                                   extent is a multiple of 64) */
+#define LBM_PLAN_PAIRED_CELLS 4u /* also use the paired two-cell step for FP32
+                                   storage (same conditions) */
 
 typedef struct {
   int32_t lattice;  /* lbm_lattice: 19 (D3Q19) or 9 (D2Q9)                */
@@ -196,8 +202,14 @@ typedef struct lbm_batch lbm_batch;
 
 typedef struct {
   int32_t blocks_per_sm; /* persistent grid = blocks_per_sm x SMs; 0 = one block per tile */
-  int32_t tile_order;    /* 0: instance after instance; 1: round-robin across instances */
+  int32_t tile_order;    /* 0: instance after instance; 1: round-robin across instances;
+                            2: instance after instance, smallest first               */
   int32_t use_graph;     /* 1: record the step sequence as a CUDA graph and replay it */
+  int32_t group_mib;     /* 0: every launch covers all instances.  > 0: consecutive
+                            instances of the tile order (0 or 2) whose two population
+                            copies fit in group_mib MiB form a group that runs all
+                            its steps before the next group starts, so a group that
+                            fits in L2 is stepped from L2 */
 } lbm_batch_config;
 
 /* plans[0..n-1] must outlive the batch and share lattice and storage. */

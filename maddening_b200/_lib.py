@@ -36,6 +36,8 @@ class LbmError(RuntimeError):
 
 
 PLAN_STAGED_ROWS = 1
+PLAN_SINGLE_CELLS = 2
+PLAN_PAIRED_CELLS = 4
 
 
 class lbm_desc(C.Structure):

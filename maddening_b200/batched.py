@@ -30,7 +30,7 @@ from .node import LBMNode
 
 class lbm_batch_config(C.Structure):
     _fields_ = [("blocks_per_sm", C.c_int32), ("tile_order", C.c_int32),
-                ("use_graph", C.c_int32)]
+                ("use_graph", C.c_int32), ("group_mib", C.c_int32)]
 
 
 _SIGS = {
@@ -54,7 +54,7 @@ def _lib_batch():
     return h
 
 
-DEFAULT_CONFIG = {"blocks_per_sm": 8, "tile_order": 0, "use_graph": 1}
+DEFAULT_CONFIG = {"blocks_per_sm": 8, "tile_order": 0, "use_graph": 1, "group_mib": 0}
 _MEM_CACHE: dict = {}
 
 
@@ -135,7 +135,7 @@ class LBMEnsemble:
         if ws is None or ws.numel() < self._ws_bytes:
             ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=dev)
         c = lbm_batch_config(int(cfg["blocks_per_sm"]), int(cfg["tile_order"]),
-                             int(cfg["use_graph"]))
+                             int(cfg["use_graph"]), int(cfg.get("group_mib", 0)))
         stream = torch.cuda.current_stream(dev).cuda_stream
         _lib.check(_lib_batch().lbm_batch_rollout(self._h, stream, f_in, f_out, int(n_steps),
                                                   args, moms, C.byref(c), ws.data_ptr(),
@@ -160,8 +160,10 @@ class LBMEnsemble:
             except (OSError, ValueError):
                 pass
         if candidates is None:
-            candidates = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g}
-                          for b in (0, 4, 8, 16) for o in (0, 1) for g in (0, 1)]
+            candidates = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g, "group_mib": 0}
+                          for b in (0, 8) for o in (0, 1) for g in (0, 1)]
+            candidates += [{"blocks_per_sm": b, "tile_order": 2, "use_graph": 1, "group_mib": m}
+                           for b in (0, 4, 8, 16) for m in (24, 48, 72, 96)]
         dev = self.nodes[0]._dev()
         ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=dev)
         timings = []

@@ -19,11 +19,13 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "liblbm_b200.so"
 SOURCES = ["lbm_abi.cu"]
-HEADERS = ["lbm_kernels.cuh", "lbm_lattice.cuh", "lbm_adjoint.cuh", "lbm_staged.cuh"]
+HEADERS = ["lbm_kernels.cuh", "lbm_lattice.cuh", "lbm_adjoint.cuh", "lbm_staged.cuh",
+           "lbm_pair.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-         "-Xcompiler", "-fPIC,-O3", "-shared", "-cudart", "static"]
+         "-Xcompiler", "-fPIC,-O3", "-shared", "-cudart", "static",
+         "--split-compile=0"]
 
 
 def nvcc() -> str:

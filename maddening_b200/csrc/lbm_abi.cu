@@ -2,6 +2,7 @@
 // mapping and kernel dispatch.  Declarations and contracts: include/lbm_b200.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -13,6 +14,7 @@
 #include "../../include/lbm_b200.h"
 #include "lbm_adjoint.cuh"
 #include "lbm_kernels.cuh"
+#include "lbm_pair.cuh"
 #include "lbm_staged.cuh"
 
 struct lbm_plan {
@@ -230,6 +232,57 @@ int launch_staged(const lbm::StepArgs& a, cudaStream_t s) {
                : launch_staged_t<Q, S, false, false, 128>(a, s);
 }
 
+// Paired-cell state step (lbm_pair.cuh): the default for 16-bit storage,
+// opt-in for FP32 (LBM_PLAN_PAIRED_CELLS), off with LBM_PLAN_SINGLE_CELLS.
+// Rows must split into whole warp segments of 64 cells; state planes and the
+// wall mask must be aligned for the pair width.
+template <class S>
+bool pair_ok(const lbm_plan* p, const lbm::StepArgs& a) {
+  if constexpr (sizeof(S) == 8) {
+    return false;
+  } else {
+    if (p->flags & LBM_PLAN_SINGLE_CELLS) return false;
+    if (sizeof(S) == 4 && !(p->flags & LBM_PLAN_PAIRED_CELLS)) return false;
+    const uintptr_t al = 2 * sizeof(S);
+    return p->g.n2 % 64 == 0 && reinterpret_cast<uintptr_t>(a.pin) % al == 0 &&
+           reinterpret_cast<uintptr_t>(a.pout) % al == 0 &&
+           reinterpret_cast<uintptr_t>(a.wall) % 2 == 0;
+  }
+}
+
+template <int Q, class S, int W>
+void launch_pair_w(const lbm::StepArgs& a, cudaStream_t s) {
+  const dim3 grid(a.g.n0 * a.g.n1, a.g.n2 / (64 * W));
+  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (faces) {
+    if (force) lbm::k_step_pair<Q, S, true, true, W><<<grid, 32 * W, 0, s>>>(a);
+    else lbm::k_step_pair<Q, S, true, false, W><<<grid, 32 * W, 0, s>>>(a);
+  } else {
+    if (force) lbm::k_step_pair<Q, S, false, true, W><<<grid, 32 * W, 0, s>>>(a);
+    else lbm::k_step_pair<Q, S, false, false, W><<<grid, 32 * W, 0, s>>>(a);
+  }
+}
+
+template <int Q, class S>
+int launch_pair(const lbm::StepArgs& a, cudaStream_t s) {
+  if constexpr (sizeof(S) == 8) {
+    return fail(LBM_ERR_UNSUPPORTED, "paired step has no FP64 form");
+  } else {
+    if (a.g.n2 % 256 == 0) launch_pair_w<Q, S, 4>(a, s);
+    else if (a.g.n2 % 128 == 0) launch_pair_w<Q, S, 2>(a, s);
+    else launch_pair_w<Q, S, 1>(a, s);
+    return cuda_check(cudaGetLastError(), "k_step_pair launch");
+  }
+}
+
+// One state-to-state step (p in -> p out, no moments): paired or one-cell.
+template <int Q, class S>
+int launch_state_step(const lbm_plan* p, const lbm::StepArgs& m, cudaStream_t s) {
+  if (pair_ok<S>(p, m)) return launch_pair<Q, S>(m, s);
+  return launch_step<Q, S>(m, false, s);
+}
+
 template <int Q, class S>
 int launch_step_moments_only(const lbm::StepArgs& a, cudaStream_t s) {
   launch_step_mode<Q, S, lbm::kOutMoments>(a, s);
@@ -260,7 +313,7 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   for (int64_t i = 0; i + 1 < n; ++i) {
     m.pin = A;
     m.pout = B;
-    rc = staged ? launch_staged<Q, S>(m, s) : launch_step<Q, S>(m, false, s);
+    rc = staged ? launch_staged<Q, S>(m, s) : launch_state_step<Q, S>(p, m, s);
     if (rc) return rc;
     char* t = A;
     A = B;
@@ -371,7 +424,7 @@ int adj_forward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* 
     char* nxt = out_for(n, cur);
     m.pin = cur;
     m.pout = nxt;
-    rc = launch_step<Q, S>(m, false, s);
+    rc = launch_state_step<Q, S>(p, m, s);
     if (rc) return rc;
     cur = nxt;
   }
@@ -496,10 +549,21 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
 // Batched ensemble (host side)
 // ---------------------------------------------------------------------------
 
+// A contiguous range [t0, t1) of the tile list whose instances are stepped
+// together; grid = blocks of the persistent launch for that range.
+struct TileRange {
+  uint32_t t0, t1;
+  unsigned grid;
+};
+
+// Prepare pass over all tiles, then for each instance group its n - 1 state
+// steps and its last step.  A group whose two population copies fit in L2
+// stays there for all of its steps.
 template <int Q, class S>
-int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t ntiles, int64_t n,
-                unsigned grid, cudaStream_t s, cudaStream_t side, bool use_graph) {
-  lbm::k_batched_prepare<Q, S><<<grid, lbm::kBlock, 0, s>>>(args, tiles, ntiles);
+int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t ntiles,
+                unsigned grid_all, const std::vector<TileRange>& groups, int64_t n,
+                cudaStream_t s, cudaStream_t side, bool use_graph) {
+  lbm::k_batched_prepare<Q, S><<<grid_all, lbm::kBlock, 0, s>>>(args, tiles, ntiles);
   int rc = cuda_check(cudaGetLastError(), "k_batched_prepare launch");
   if (rc) return rc;
   cudaStream_t ls = s;
@@ -513,10 +577,14 @@ int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t
     if (rc) return rc;
     ls = side;
   }
-  for (int64_t k = 1; k < n; ++k)
-    lbm::k_batched_step<Q, S, lbm::kOutState><<<grid, lbm::kBlock, 0, ls>>>(
-        args, tiles, ntiles, static_cast<int>(k % 2));
-  lbm::k_batched_step<Q, S, lbm::kOutAoS><<<grid, lbm::kBlock, 0, ls>>>(args, tiles, ntiles, 2);
+  for (const TileRange& r : groups) {
+    const lbm::BatchTile* t = tiles + r.t0;
+    const uint32_t nt = r.t1 - r.t0;
+    for (int64_t k = 1; k < n; ++k)
+      lbm::k_batched_step<Q, S, lbm::kOutState><<<r.grid, lbm::kBlock, 0, ls>>>(
+          args, t, nt, static_cast<int>(k % 2));
+    lbm::k_batched_step<Q, S, lbm::kOutAoS><<<r.grid, lbm::kBlock, 0, ls>>>(args, t, nt, 2);
+  }
   rc = cuda_check(cudaGetLastError(), "k_batched_step launch");
   if (use_graph) {
     const int rc2 = cuda_check(cudaStreamEndCapture(side, &graph), "cudaStreamEndCapture");
@@ -534,12 +602,19 @@ int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t
 
 }  // namespace
 
+constexpr int kTileOrders = 3;
+
 struct lbm_batch {
   int n = 0, Q = 0, D = 0, storage = 0;
   std::vector<const lbm_plan*> plans;
   std::vector<size_t> state_off;  // instance i: two population copies at this offset
-  size_t args_off = 0, tiles_off[2] = {0, 0}, total = 0;
-  std::vector<lbm::BatchTile> tiles[2];  // [0] instance-major, [1] round-robin
+  size_t args_off = 0, tiles_off[kTileOrders] = {0, 0, 0}, total = 0;
+  // [0] instance-major in member order, [1] round-robin across members,
+  // [2] instance-major from the smallest member to the largest
+  std::vector<lbm::BatchTile> tiles[kTileOrders];
+  // members in the order of tile lists 0 and 2, with their first tile
+  std::vector<int> order[kTileOrders];
+  std::vector<uint32_t> first_tile[kTileOrders];
   cudaStream_t side = nullptr;
 };
 
@@ -808,14 +883,25 @@ int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
     delete b;
     return fail(LBM_ERR_INVALID, "ensemble too large");
   }
-  for (int i = 0; i < n; ++i) b->tiles[0].insert(b->tiles[0].end(), per[i].begin(), per[i].end());
+  std::vector<int> by_size(n);
+  for (int i = 0; i < n; ++i) by_size[i] = i;
+  std::stable_sort(by_size.begin(), by_size.end(),
+                   [&](int x, int y) { return plans[x]->g.ncell < plans[y]->g.ncell; });
+  for (int k : {0, 2}) {
+    for (int j = 0; j < n; ++j) {
+      const int i = k == 0 ? j : by_size[j];
+      b->order[k].push_back(i);
+      b->first_tile[k].push_back(static_cast<uint32_t>(b->tiles[k].size()));
+      b->tiles[k].insert(b->tiles[k].end(), per[i].begin(), per[i].end());
+    }
+  }
   for (size_t r = 0;; ++r) {  // round-robin across instances
     bool any = false;
     for (int i = 0; i < n; ++i)
       if (r < per[i].size()) { b->tiles[1].push_back(per[i][r]); any = true; }
     if (!any) break;
   }
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < kTileOrders; ++k) {
     b->tiles_off[k] = o;
     o += align256(sizeof(lbm::BatchTile) * ntiles);
   }
@@ -851,10 +937,12 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
   if (workspace == nullptr || workspace_bytes < b->total)
     return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", b->total,
                 workspace_bytes);
-  lbm_batch_config c{0, 0, 0};
+  lbm_batch_config c{0, 0, 0, 0};
   if (cfg != nullptr) c = *cfg;
-  if (c.tile_order < 0 || c.tile_order > 1 || c.blocks_per_sm < 0)
+  if (c.tile_order < 0 || c.tile_order >= kTileOrders || c.blocks_per_sm < 0 || c.group_mib < 0)
     return fail(LBM_ERR_INVALID, "bad batch config");
+  if (c.group_mib > 0 && c.tile_order == 1)
+    return fail(LBM_ERR_INVALID, "instance groups need an instance-major tile order (0 or 2)");
   if (c.use_graph && b->side == nullptr)
     return fail(LBM_ERR_UNSUPPORTED, "no capture stream for CUDA-graph replay");
   char* ws = static_cast<char*>(workspace);
@@ -893,29 +981,49 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
                                   cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
   if (rc) return rc;
   const uint32_t ntiles = static_cast<uint32_t>(tl.size());
-  unsigned grid = ntiles;
+  unsigned cap = 0;  // persistent grid size, 0 = one block per tile
   if (c.blocks_per_sm > 0) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    grid = static_cast<unsigned>(c.blocks_per_sm) * static_cast<unsigned>(sms);
-    if (grid > ntiles) grid = ntiles;
+    cap = static_cast<unsigned>(c.blocks_per_sm) * static_cast<unsigned>(sms);
   }
+  auto grid_for_tiles = [cap](uint32_t nt) { return cap > 0 && cap < nt ? cap : nt; };
+  // Instance groups: consecutive members of the tile order whose two
+  // population copies together stay within group_mib (a member larger than
+  // that is a group of its own); 0 = all members in every launch.
+  std::vector<TileRange> groups;
+  if (c.group_mib == 0) {
+    groups.push_back(TileRange{0, ntiles, grid_for_tiles(ntiles)});
+  } else {
+    const size_t budget = static_cast<size_t>(c.group_mib) << 20;
+    const auto& ord = b->order[c.tile_order];
+    const auto& ft = b->first_tile[c.tile_order];
+    size_t used = 0;
+    uint32_t t0 = 0;
+    for (size_t j = 0; j < ord.size(); ++j) {
+      const size_t need = 2 * align256(state_bytes(b->plans[ord[j]]));
+      if (j > 0 && used + need > budget) {
+        groups.push_back(TileRange{t0, ft[j], grid_for_tiles(ft[j] - t0)});
+        t0 = ft[j];
+        used = 0;
+      }
+      used += need;
+    }
+    groups.push_back(TileRange{t0, ntiles, grid_for_tiles(ntiles - t0)});
+  }
+  const unsigned grid_all = grid_for_tiles(ntiles);
   const bool g = c.use_graph != 0;
+#define LBM_BATCH_RUN(QQ, SS) \
+  batched_run<QQ, SS>(dargs, dtiles, ntiles, grid_all, groups, n_steps, s, b->side, g)
   switch (b->storage) {
-    case LBM_STORE_F32:
-      return b->Q == 19 ? batched_run<19, float>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
-                        : batched_run<9, float>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
-    case LBM_STORE_F16:
-      return b->Q == 19 ? batched_run<19, __half>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
-                        : batched_run<9, __half>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
+    case LBM_STORE_F32: return b->Q == 19 ? LBM_BATCH_RUN(19, float) : LBM_BATCH_RUN(9, float);
+    case LBM_STORE_F16: return b->Q == 19 ? LBM_BATCH_RUN(19, __half) : LBM_BATCH_RUN(9, __half);
     case LBM_STORE_BF16:
-      return b->Q == 19 ? batched_run<19, __nv_bfloat16>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
-                        : batched_run<9, __nv_bfloat16>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
-    case LBM_STORE_F64:
-      return b->Q == 19 ? batched_run<19, double>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g)
-                        : batched_run<9, double>(dargs, dtiles, ntiles, n_steps, grid, s, b->side, g);
+      return b->Q == 19 ? LBM_BATCH_RUN(19, __nv_bfloat16) : LBM_BATCH_RUN(9, __nv_bfloat16);
+    case LBM_STORE_F64: return b->Q == 19 ? LBM_BATCH_RUN(19, double) : LBM_BATCH_RUN(9, double);
   }
+#undef LBM_BATCH_RUN
   return fail(LBM_ERR_INVALID, "bad storage");
 }
 

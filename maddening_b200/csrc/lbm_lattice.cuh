@@ -38,6 +38,9 @@ struct Lat<19> {
   __host__ __device__ static constexpr double w(int q) {
     return q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
   }
+  // w(q) = wr(q) / kWDen with integer wr
+  static constexpr int kWDen = 36;
+  __host__ __device__ static constexpr int wr(int q) { return q == 0 ? 12 : (q <= 6 ? 2 : 1); }
 };
 
 template <>
@@ -59,6 +62,8 @@ struct Lat<9> {
   __host__ __device__ static constexpr double w(int q) {
     return q == 0 ? 4.0 / 9.0 : (q <= 4 ? 1.0 / 9.0 : 1.0 / 36.0);
   }
+  static constexpr int kWDen = 36;
+  __host__ __device__ static constexpr int wr(int q) { return q == 0 ? 16 : (q <= 4 ? 4 : 1); }
 };
 
 // Component of direction q along internal axis a (a is a runtime value).

@@ -1,0 +1,212 @@
+// Paired-cell fused step: each thread updates two neighbouring cells (k, k+1)
+// of one row, reading and writing every population plane as one 32-bit word
+// (two 16-bit offsets) or one 64-bit word (two FP32 offsets).
+//
+// Why: with 16-bit storage a one-cell-per-thread step keeps only 19 x 2 B of
+// loads in flight per thread, too little to cover HBM latency at the
+// occupancy its registers allow, and it spends an address computation, a
+// conversion and a memory instruction on every 2-byte value.  Pairs double
+// the bytes in flight per thread, pack each output pair with one conversion
+// and halve the memory instructions.
+//
+// Block layout: a block of W warps covers 64 W consecutive cells of one row
+// (blockIdx.x = row i0 * n1 + i1, blockIdx.y = segment along the row), so the
+// row coordinates and the 19 source-row base pointers are block-uniform.  Lane
+// l of a warp owns the aligned pair (k, k+1), k = first + 2 l.  The pull
+// along the contiguous axis:
+//   c2 =  0: both cells read the thread's own pair;
+//   c2 = +1: cell k reads k - 1, the high half of lane l-1's pair (shuffle
+//            up); lane 0 loads the pair before the warp's segment itself
+//            (periodic wrap at the row start); cell k+1 reads the low half of
+//            its own pair;
+//   c2 = -1: mirror image (shuffle down; lane 31 loads the pair after).
+// After the pull each cell runs exactly the arithmetic of the one-cell step
+// (wall swap -> faces -> moments -> collide), so the results are
+// bit-identical; the wall swap is skipped by warps without a wall cell and the
+// face checks by pairs that cannot touch a face.
+//
+// Requirements (checked on the host): n2 a multiple of 64 W, state planes and
+// the wall mask aligned for the pair width.  Used for the state-to-state steps
+// of a rollout; the other modes keep the one-cell kernels.
+#pragma once
+
+#include "lbm_kernels.cuh"
+
+namespace lbm {
+
+template <class S>
+struct PairT;
+
+template <>
+struct PairT<__half> {
+  using P = uint32_t;
+  static __device__ __forceinline__ P ld(const __half* p) {
+    return __ldg(reinterpret_cast<const unsigned int*>(p));
+  }
+  static __device__ __forceinline__ float lo(P v) {
+    return __low2float(*reinterpret_cast<const __half2*>(&v));
+  }
+  static __device__ __forceinline__ float hi(P v) {
+    return __high2float(*reinterpret_cast<const __half2*>(&v));
+  }
+  static __device__ __forceinline__ P shup(P v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+  static __device__ __forceinline__ P shdn(P v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+  static __device__ __forceinline__ void st(__half* p, float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    *reinterpret_cast<unsigned int*>(p) = *reinterpret_cast<const unsigned int*>(&h);
+  }
+};
+
+template <>
+struct PairT<__nv_bfloat16> {
+  using P = uint32_t;
+  static __device__ __forceinline__ P ld(const __nv_bfloat16* p) {
+    return __ldg(reinterpret_cast<const unsigned int*>(p));
+  }
+  static __device__ __forceinline__ float lo(P v) { return __uint_as_float(v << 16); }
+  static __device__ __forceinline__ float hi(P v) { return __uint_as_float(v & 0xffff0000u); }
+  static __device__ __forceinline__ P shup(P v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+  static __device__ __forceinline__ P shdn(P v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+  static __device__ __forceinline__ void st(__nv_bfloat16* p, float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    *reinterpret_cast<unsigned int*>(p) = *reinterpret_cast<const unsigned int*>(&h);
+  }
+};
+
+template <>
+struct PairT<float> {
+  using P = float2;
+  static __device__ __forceinline__ P ld(const float* p) {
+    return __ldg(reinterpret_cast<const float2*>(p));
+  }
+  static __device__ __forceinline__ float lo(P v) { return v.x; }
+  static __device__ __forceinline__ float hi(P v) { return v.y; }
+  static __device__ __forceinline__ P shup(P v) {
+    return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
+  }
+  static __device__ __forceinline__ P shdn(P v) {
+    return make_float2(__shfl_down_sync(0xffffffffu, v.x, 1),
+                       __shfl_down_sync(0xffffffffu, v.y, 1));
+  }
+  static __device__ __forceinline__ void st(float* p, float a, float b) {
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+  }
+};
+
+#ifndef LBM_PAIR_MIN_WARPS
+#define LBM_PAIR_MIN_WARPS 24
+#endif
+// Resident warps per SM the register budget is set for.
+constexpr int kPairMinWarps = LBM_PAIR_MIN_WARPS;
+
+// Moments and collide of one cell whose f_bc populations are in d.
+template <int Q, class S, bool FORCE>
+__device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, float (&d)[Q]) {
+  using IO = typename StoreT<S>::IO;
+  float F[3] = {0, 0, 0};
+  if (FORCE) {
+    if (a.force_mode == 2) load_force<Q, IO>(a.force_field, x.c, F);
+    else uniform_force<Q, float>(a, F);
+  }
+  const Mom<float> m = moments<Q, float, FORCE>(d, F);
+  collide<Q, float, FORCE>(d, m, F, static_cast<float>(a.omega), static_cast<float>(a.guo_c));
+}
+
+template <int Q, class S, bool FACES, bool FORCE, int W>
+__global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
+    k_step_pair(const __grid_constant__ StepArgs a) {
+  using PT = PairT<S>;
+  using P = typename PT::P;
+  const Geo& g = a.g;
+  const uint32_t row = blockIdx.x;
+  const uint32_t i0 = fdiv(row, g.div_n1);
+  const uint32_t i1 = row - i0 * g.n1;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t wfirst = blockIdx.y * (64u * W) + (threadIdx.x >> 5) * 64u;
+  const uint32_t k = wfirst + 2u * lane;
+  // pair before / after this warp's segment (periodic along the row)
+  const uint32_t kprev = (wfirst == 0 ? g.n2 : wfirst) - 2u;
+  const uint32_t knext = wfirst + 64u == g.n2 ? 0u : wfirst + 64u;
+  // source rows of the pull x - e_q (periodic)
+  const uint32_t i0m = i0 == 0 ? g.n0 - 1 : i0 - 1, i0p = i0 + 1 == g.n0 ? 0u : i0 + 1;
+  const uint32_t i1m = i1 == 0 ? g.n1 - 1 : i1 - 1, i1p = i1 + 1 == g.n1 ? 0u : i1 + 1;
+
+  const S* pin = static_cast<const S*>(a.pin);
+  P v[Q];
+  P e[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
+    const uint32_t s0 = c0 > 0 ? i0m : (c0 < 0 ? i0p : i0);
+    const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
+    const S* base = pin + (static_cast<uint32_t>(q) * g.ncell + (s0 * g.n1 + s1) * g.n2);
+    v[q] = PT::ld(base + k);
+    if (c2 > 0 && lane == 0) e[q] = PT::ld(base + kprev);
+    if (c2 < 0 && lane == 31) e[q] = PT::ld(base + knext);
+  }
+  float da[Q], db[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c2 = Lat<Q>::c2(q);
+    if (c2 == 0) {
+      da[q] = PT::lo(v[q]);
+      db[q] = PT::hi(v[q]);
+    } else if (c2 > 0) {
+      P nb = PT::shup(v[q]);
+      if (lane == 0) nb = e[q];
+      da[q] = PT::hi(nb);
+      db[q] = PT::lo(v[q]);
+    } else {
+      P nb = PT::shdn(v[q]);
+      if (lane == 31) nb = e[q];
+      da[q] = PT::hi(v[q]);
+      db[q] = PT::lo(nb);
+    }
+  }
+  const uint32_t rbase = row * g.n2;
+  bool wa = false, wb = false;
+  if (a.wall != nullptr) {
+    const uint32_t w2 = __ldg(reinterpret_cast<const unsigned short*>(a.wall + rbase + k));
+    wa = (w2 & 0xffu) != 0;
+    wb = (w2 >> 8) != 0;
+  }
+  Cell xa, xb;
+  xa.c = rbase + k;
+  xa.i0 = i0;
+  xa.i1 = i1;
+  xa.k = k;
+  xa.row = rbase;
+  xb = xa;
+  xb.c = xa.c + 1;
+  xb.k = k + 1;
+  // Wall swap only in warps that hold a wall cell (obstacles are clustered).
+  if (__any_sync(0xffffffffu, wa || wb)) {
+    if (wa) wall_swap<Q>(da);
+    if (wb) wall_swap<Q>(db);
+  }
+  if constexpr (FACES) {
+    // Face rows (axes 0 and 1) are block-uniform; on the contiguous axis only
+    // the first and the last pair of a row can hold a face cell.
+    bool near = false;
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+      const FaceK& fc = a.face[fi];
+      if (fc.kind == kFaceNone) continue;
+      if (fc.axis == 0) near |= i0 == (fc.side == 0 ? 0u : g.n0 - 1);
+      else if (fc.axis == 1) near |= i1 == (fc.side == 0 ? 0u : g.n1 - 1);
+      else near |= fc.side == 0 ? k == 0 : k + 2 == g.n2;
+    }
+    if (near) {
+      if (!wa) apply_faces<Q, S>(a, xa, da);
+      if (!wb) apply_faces<Q, S>(a, xb, db);
+    }
+  }
+  pair_cell<Q, S, FORCE>(a, xa, da);
+  pair_cell<Q, S, FORCE>(a, xb, db);
+  S* pout = static_cast<S*>(a.pout);
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+    PT::st(pout + (static_cast<uint32_t>(q) * g.ncell + rbase + k), da[q], db[q]);
+}
+
+}  // namespace lbm

@@ -17,6 +17,10 @@ Additions beyond the reference (documented extensions):
 * ``storage`` -- how populations are held between steps inside ``run``:
   ``"f32"`` (default), ``"f16"``/``"bf16"`` (normalised offsets, FP32
   arithmetic) or ``"f64"`` (FP64 throughout; state arrays are float64).
+* ``cells_per_thread`` -- kernel form of the steps inside ``run``: ``None``
+  (default: two neighbouring cells per thread for FP16/BF16 storage when the
+  contiguous extent is a multiple of 64, else one), ``1`` or ``2`` (also for
+  FP32).  Every form gives bit-identical results.
 """
 
 from __future__ import annotations
@@ -85,7 +89,8 @@ class LBMNode(SimulationNode):
                  wall_mask: Optional[np.ndarray] = None, inlet_face: str = "x_min",
                  outlet_face: str = "x_max", geometry_source: Optional[str] = None,
                  *, outlet_condition: str = "pressure", storage: str = "f32",
-                 device=None, staged_rows: bool = False):
+                 device=None, staged_rows: bool = False,
+                 cells_per_thread: Optional[int] = None):
         lat = by_name(lattice)
         if len(grid_shape) != lat.D:
             raise ValueError(f"grid_shape has {len(grid_shape)} dims but lattice "
@@ -131,8 +136,14 @@ class LBMNode(SimulationNode):
             self._wall_np = np.zeros(self._grid_shape, dtype=bool)
         self._has_walls = bool(self._wall_np.any())
         self._wall_dev = {}
-        self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage,
-                               _lib.PLAN_STAGED_ROWS if staged_rows else 0)
+        if cells_per_thread not in (None, 1, 2):
+            raise ValueError(f"cells_per_thread must be None, 1 or 2 (got {cells_per_thread})")
+        flags = _lib.PLAN_STAGED_ROWS if staged_rows else 0
+        if cells_per_thread == 1:
+            flags |= _lib.PLAN_SINGLE_CELLS
+        elif cells_per_thread == 2:
+            flags |= _lib.PLAN_PAIRED_CELLS
+        self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage, flags)
 
     # -- properties (lbm.py:690-703) ---------------------------------------
     @property

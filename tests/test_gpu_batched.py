@@ -50,8 +50,10 @@ def _members(storage="f32", lattice="D3Q19"):
     return nodes, bis, states
 
 
-CONFIGS = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g}
-           for b, o, g in ((0, 0, 0), (8, 0, 1), (4, 1, 0), (16, 1, 1), (1, 0, 1))]
+CONFIGS = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g, "group_mib": m}
+           for b, o, g, m in ((0, 0, 0, 0), (8, 0, 1, 0), (4, 1, 0, 0), (16, 1, 1, 0),
+                              (1, 0, 1, 0), (8, 2, 1, 1), (0, 0, 0, 1), (4, 2, 0, 4096),
+                              (0, 2, 1, 0))]
 
 
 @pytest.mark.parametrize("lattice", ["D3Q19", "D2Q9"])
@@ -67,6 +69,16 @@ def test_batched_members_equal_their_own_rollouts(lattice, storage):
         for i, (o, r) in enumerate(zip(out, ref)):
             for key in ("f", "density", "velocity", "pressure"):
                 assert torch.equal(o[key], r[key]), (cfg, i, key)
+
+
+def test_grouped_launch_rejects_round_robin_order():
+    from maddening_b200 import _lib
+    from maddening_b200.batched import LBMEnsemble
+    nodes, bis, states = _members()
+    ens = LBMEnsemble(nodes)
+    with pytest.raises(_lib.LbmError, match="instance-major"):
+        ens.run(states, bis, 2, {"blocks_per_sm": 0, "tile_order": 1, "use_graph": 0,
+                                 "group_mib": 8})
 
 
 def test_batched_member_matches_fp64_oracle():
@@ -89,8 +101,9 @@ def test_autotune_picks_a_valid_config():
     nodes, bis, states = _members()
     ens = LBMEnsemble(nodes)
     cfg = ens.autotune(states, bis, n_steps=4, use_cache=False)
-    assert cfg in [{"blocks_per_sm": b, "tile_order": o, "use_graph": g}
-                   for b in (0, 4, 8, 16) for o in (0, 1) for g in (0, 1)]
+    assert set(cfg) == {"blocks_per_sm", "tile_order", "use_graph", "group_mib"}
+    assert cfg["blocks_per_sm"] in (0, 4, 8, 16) and cfg["tile_order"] in (0, 1, 2)
+    assert cfg["use_graph"] in (0, 1) and cfg["group_mib"] >= 0
     ref = [n.run(s, b, 3) for n, s, b in zip(nodes, states, bis)]
     out = ens.run(states, bis, 3)
     for o, r in zip(out, ref):
