@@ -287,18 +287,23 @@ def run_ours(args):
             torch.cuda.synchronize()
             a0 = torch.cuda.Event(enable_timing=True)
             a1 = torch.cuda.Event(enable_timing=True)
-            nv = min(K, 200)
             a0.record(stream)
-            vn.run(vs, bi, nv)
+            vn.run(vs, bi, K)
             a1.record(stream)
             torch.cuda.synchronize()
             tv = a0.elapsed_time(a1) / 1e3
-            variants[storage] = {"mlups": round(cells * nv / tv / 1e6, 1), "steps": nv,
-                                 "bytes_per_cell": 76}
+            mv = cells * K / tv / 1e6
+            variants[storage] = {"mlups": round(mv, 1), "steps": K, "bytes_per_cell": 76,
+                                 "over_fp32": round(mv / (mlups / world), 3),
+                                 "hbm_frac": round(mv * 1e6 * 76 / 1e9 / _peaks()[0], 4)}
             del vn, vs
+        torch.cuda.empty_cache()
 
     if not args.no_variants and rank == 0:
+        variants["precision_512"] = precision_cost(dev, args.c5_steps)
+        torch.cuda.empty_cache()
         variants["adjoint"] = adjoint_cost(dev)
+        torch.cuda.empty_cache()
         variants["batched"] = batched_cost(dev)
 
     if rank == 0:
@@ -339,6 +344,59 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def precision_cost(dev, steps):
+    """512^3 D3Q19 obstacle flow (the 256^3 workload's generator: spheres of
+    radii 4-12, 10 % solid; velocity inlet 0.05, zero-gradient outlet, tau 0.6),
+    `steps` steps with populations stored as FP64 (the reference run, FP64
+    arithmetic), FP32, FP16 and BF16 offsets (FP32 arithmetic).  Reports MLUPS
+    of each and the relative L2 error of density, density - 1 and velocity
+    against the FP64 run, computed on the device."""
+    import torch
+    from maddening_b200 import LBMNode
+    from maddening_b200.geometry import random_spheres
+    grid = (512, 512, 512)
+    cells = grid[0] * grid[1] * grid[2]
+    wall = random_spheres(grid, seed=0)
+    bi = {"inlet_velocity": np.array(U_IN)}
+    out, ref = {}, None
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm((a.double() - b).flatten())
+                     / torch.linalg.vector_norm(b.flatten()))
+
+    for storage in ("f64", "f32", "f16", "bf16"):
+        node = LBMNode("p", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0, wall_mask=wall,
+                       outlet_condition="zero_gradient", storage=storage, device=dev)
+        st = node.initial_state()
+        node.run(st, bi, 2)  # warm-up
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = node.run(st, bi, steps)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        entry = {"mlups": round(cells * steps / t / 1e6, 1)}
+        rho, vel = res["density"], res["velocity"]
+        del res, st, node
+        torch.cuda.empty_cache()
+        if storage == "f64":
+            ref = (rho, vel)
+        else:
+            entry["relL2_rho"] = float(f"{rel(rho, ref[0]):.3e}")
+            entry["relL2_rho_minus_1"] = float(f"{rel(rho - 1.0, ref[0] - 1.0):.3e}")
+            entry["relL2_u"] = float(f"{rel(vel, ref[1]):.3e}")
+            del rho, vel
+        out[storage] = entry
+    for storage in ("f16", "bf16"):
+        out[storage]["over_fp32"] = round(out[storage]["mlups"] / out["f32"]["mlups"], 3)
+    del ref
+    torch.cuda.empty_cache()
+    return {"workload": f"512^3 D3Q19 obstacle flow, {steps} steps, errors vs the FP64 "
+                        "storage run", **out}
 
 
 def batched_cost(dev, steps=500):
@@ -458,6 +516,8 @@ def main():
                     help="population storage of the measured run (default f32)")
     ap.add_argument("--grid", type=int, default=256,
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
+    ap.add_argument("--c5-steps", type=int, default=2000,
+                    help="steps of the 512^3 precision comparison (variants)")
     args = ap.parse_args()
     global GRID
     GRID = (args.grid,) * 3

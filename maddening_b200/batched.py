@@ -54,7 +54,7 @@ def _lib_batch():
     return h
 
 
-DEFAULT_CONFIG = {"blocks_per_sm": 8, "tile_order": 0, "use_graph": 1, "group_mib": 0}
+DEFAULT_CONFIG = {"blocks_per_sm": 0, "tile_order": 0, "use_graph": 1, "group_mib": 0}
 _MEM_CACHE: dict = {}
 
 
@@ -161,9 +161,9 @@ class LBMEnsemble:
                 pass
         if candidates is None:
             candidates = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g, "group_mib": 0}
-                          for b in (0, 8) for o in (0, 1) for g in (0, 1)]
+                          for b in (0, 4, 8, 16) for o in (0, 1) for g in (0, 1)]
             candidates += [{"blocks_per_sm": b, "tile_order": 2, "use_graph": 1, "group_mib": m}
-                           for b in (0, 4, 8, 16) for m in (24, 48, 72, 96)]
+                           for b in (0, 8) for m in (48, 96)]
         dev = self.nodes[0]._dev()
         ws = torch.empty(self._ws_bytes, dtype=torch.uint8, device=dev)
         timings = []

@@ -559,10 +559,29 @@ struct TileRange {
 // Prepare pass over all tiles, then for each instance group its n - 1 state
 // steps and its last step.  A group whose two population copies fit in L2
 // stays there for all of its steps.
+template <int Q, class S, int MODE, int SPEC>
+void batched_launch(const lbm::StepArgs* args, const lbm::BatchTile* t, uint32_t nt, unsigned grid,
+                    int which, cudaStream_t s) {
+  lbm::k_batched_step<Q, S, MODE, SPEC><<<grid, lbm::kBlock, 0, s>>>(args, t, nt, which);
+}
+
+// spec: 0 = per-tile run-time choice, else 1 + 2 FACES + FORCE shared by all members
+template <int Q, class S, int MODE>
+void batched_step(int spec, const lbm::StepArgs* args, const lbm::BatchTile* t, uint32_t nt,
+                  unsigned grid, int which, cudaStream_t s) {
+  switch (spec) {
+    case 1: batched_launch<Q, S, MODE, 1>(args, t, nt, grid, which, s); break;
+    case 2: batched_launch<Q, S, MODE, 2>(args, t, nt, grid, which, s); break;
+    case 3: batched_launch<Q, S, MODE, 3>(args, t, nt, grid, which, s); break;
+    case 4: batched_launch<Q, S, MODE, 4>(args, t, nt, grid, which, s); break;
+    default: batched_launch<Q, S, MODE, 0>(args, t, nt, grid, which, s); break;
+  }
+}
+
 template <int Q, class S>
 int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t ntiles,
                 unsigned grid_all, const std::vector<TileRange>& groups, int64_t n,
-                cudaStream_t s, cudaStream_t side, bool use_graph) {
+                cudaStream_t s, cudaStream_t side, bool use_graph, int spec) {
   lbm::k_batched_prepare<Q, S><<<grid_all, lbm::kBlock, 0, s>>>(args, tiles, ntiles);
   int rc = cuda_check(cudaGetLastError(), "k_batched_prepare launch");
   if (rc) return rc;
@@ -581,9 +600,8 @@ int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t
     const lbm::BatchTile* t = tiles + r.t0;
     const uint32_t nt = r.t1 - r.t0;
     for (int64_t k = 1; k < n; ++k)
-      lbm::k_batched_step<Q, S, lbm::kOutState><<<r.grid, lbm::kBlock, 0, ls>>>(
-          args, t, nt, static_cast<int>(k % 2));
-    lbm::k_batched_step<Q, S, lbm::kOutAoS><<<r.grid, lbm::kBlock, 0, ls>>>(args, t, nt, 2);
+      batched_step<Q, S, lbm::kOutState>(spec, args, t, nt, r.grid, static_cast<int>(k % 2), ls);
+    batched_step<Q, S, lbm::kOutAoS>(spec, args, t, nt, r.grid, 2, ls);
   }
   rc = cuda_check(cudaGetLastError(), "k_batched_step launch");
   if (use_graph) {
@@ -875,7 +893,7 @@ int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
       return fail(LBM_ERR_INVALID, "instance %d: plans must share lattice and storage", i);
     }
     b->plans.push_back(p);
-    for (uint32_t c = 0; c < p->g.ncell; c += lbm::kBlock)
+    for (uint32_t c = 0; c < p->g.ncell; c += lbm::kBatchTile)
       per[i].push_back(lbm::BatchTile{static_cast<uint32_t>(i), c});
     ntiles += per[i].size();
   }
@@ -970,6 +988,14 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
     h[2].pin = n_steps % 2 == 1 ? A : B;
     h[2].f_out = f_out[i];
   }
+  // One face / force specialisation shared by every member: compile-time kernel.
+  int spec = -1;
+  for (int i = 0; i < b->n; ++i) {
+    const lbm::StepArgs& h = host[static_cast<size_t>(lbm::kBatchArgs) * i];
+    const bool faces = h.face[0].kind != lbm::kFaceNone || h.face[1].kind != lbm::kFaceNone;
+    const int si = 1 + 2 * (faces ? 1 : 0) + (h.force_mode != 0 ? 1 : 0);
+    spec = spec < 0 || spec == si ? si : 0;
+  }
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   lbm::StepArgs* dargs = reinterpret_cast<lbm::StepArgs*>(ws + b->args_off);
   lbm::BatchTile* dtiles = reinterpret_cast<lbm::BatchTile*>(ws + b->tiles_off[c.tile_order]);
@@ -1015,7 +1041,7 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
   const unsigned grid_all = grid_for_tiles(ntiles);
   const bool g = c.use_graph != 0;
 #define LBM_BATCH_RUN(QQ, SS) \
-  batched_run<QQ, SS>(dargs, dtiles, ntiles, grid_all, groups, n_steps, s, b->side, g)
+  batched_run<QQ, SS>(dargs, dtiles, ntiles, grid_all, groups, n_steps, s, b->side, g, spec)
   switch (b->storage) {
     case LBM_STORE_F32: return b->Q == 19 ? LBM_BATCH_RUN(19, float) : LBM_BATCH_RUN(9, float);
     case LBM_STORE_F16: return b->Q == 19 ? LBM_BATCH_RUN(19, __half) : LBM_BATCH_RUN(9, __half);

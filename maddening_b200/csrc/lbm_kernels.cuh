@@ -552,7 +552,10 @@ __device__ __forceinline__ void apply_faces(const StepArgs& a, const Cell& x,
 template <int Q, class S, bool FACES>
 __device__ __forceinline__ void apply_bc(const StepArgs& a, const Cell& x, bool wall,
                                          typename StoreT<S>::R (&d)[Q]) {
-  if (wall) wall_swap<Q>(d);
+  // Obstacles are clustered: most warps hold no wall cell and skip the swap.
+  if (__any_sync(__activemask(), wall)) {
+    if (wall) wall_swap<Q>(d);
+  }
   // wall face cells keep the swapped populations
   if constexpr (FACES) {
     if (!wall) apply_faces<Q, S>(a, x, d);
@@ -592,13 +595,11 @@ __device__ __forceinline__ void finish_cell(const StepArgs& a, const Cell& x,
   }
 }
 
-// One fused step of cell cidx: pull p from global memory, then finish_cell.
-template <int Q, class S, int MODE, bool FACES, bool FORCE>
-__device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
-  using R = typename StoreT<S>::R;
+// The pulled populations p(x - e_q) of cell x (periodic on every axis).
+template <int Q, class S>
+__device__ __forceinline__ void pull_cell(const StepArgs& a, const Cell& x,
+                                          typename StoreT<S>::R (&d)[Q]) {
   const Geo& g = a.g;
-  const Cell x = locate(g, cidx);
-
   // Offsets of the source rows of the pull x - e_q (periodic on every axis).
   const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
   const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
@@ -607,7 +608,6 @@ __device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
   const uint32_t km = x.k == 0 ? g.n2 - 1 : x.k - 1;
   const uint32_t kp = x.k == g.n2 - 1 ? 0 : x.k + 1;
 
-  R d[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
@@ -619,6 +619,15 @@ __device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
     off += c2 > 0 ? km : (c2 < 0 ? kp : x.k);
     d[q] = ld_pop<S>(static_cast<const S*>(a.pin) + (static_cast<uint32_t>(q) * g.ncell + off));
   }
+}
+
+// One fused step of cell cidx: pull p from global memory, then finish_cell.
+template <int Q, class S, int MODE, bool FACES, bool FORCE>
+__device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
+  using R = typename StoreT<S>::R;
+  const Cell x = locate(a.g, cidx);
+  R d[Q];
+  pull_cell<Q, S>(a, x, d);
   finish_cell<Q, S, MODE, FACES, FORCE>(a, x, d);
 }
 
@@ -633,7 +642,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
 // Batched ensemble: many lattices (own shape, tau, force, walls) in one launch
 // ---------------------------------------------------------------------------
 
-// A tile is kBlock consecutive cells of one instance.
+// A tile is kBatchTile consecutive cells of one instance.
+constexpr int kBatchTile = 2 * kBlock;
 struct BatchTile {
   uint32_t inst;
   uint32_t first;
@@ -667,8 +677,11 @@ __device__ __forceinline__ void step_cell_any(const StepArgs& a, uint32_t c) {
 }
 
 // Persistent launch: each block walks the tile list with a grid stride; tile
-// t uses args[kBatchArgs * inst + which], staged in shared memory.
-template <int Q, class S, int MODE>
+// t uses args[kBatchArgs * inst + which], staged in shared memory.  SPEC = 0:
+// every member's face / force specialisation is chosen per tile at run time;
+// otherwise all members share the one given at compile time (SPEC = 1 +
+// 2 FACES + FORCE), which keeps a single copy of the step body in the kernel.
+template <int Q, class S, int MODE, int SPEC>
 __global__ void __launch_bounds__(kBlock, min_blocks<S>())
     k_batched_step(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                    uint32_t ntiles, int which) {
@@ -682,8 +695,13 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
       __syncthreads();
       cur = tile.inst;
     }
-    const uint32_t c = tile.first + threadIdx.x;
-    if (c < sa.g.ncell) step_cell_any<Q, S, MODE>(sa, c);
+#pragma unroll 1
+    for (int j = 0; j < kBatchTile / kBlock; ++j) {
+      const uint32_t c = tile.first + j * kBlock + threadIdx.x;
+      if (c >= sa.g.ncell) break;
+      if constexpr (SPEC == 0) step_cell_any<Q, S, MODE>(sa, c);
+      else step_cell<Q, S, MODE, ((SPEC - 1) & 2) != 0, ((SPEC - 1) & 1) != 0>(sa, c);
+    }
   }
 }
 
@@ -701,10 +719,13 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
       __syncthreads();
       cur = tile.inst;
     }
-    const uint32_t c = tile.first + threadIdx.x;
-    if (c < sa.g.ncell) {
-      if (sa.force_mode != 0) prepare_cell<Q, S, true>(sa, c);
-      else prepare_cell<Q, S, false>(sa, c);
+#pragma unroll 1
+    for (int j = 0; j < 2; ++j) {
+      const uint32_t c = tile.first + j * kBlock + threadIdx.x;
+      if (c < sa.g.ncell) {
+        if (sa.force_mode != 0) prepare_cell<Q, S, true>(sa, c);
+        else prepare_cell<Q, S, false>(sa, c);
+      }
     }
   }
 }

@@ -71,6 +71,22 @@ def test_batched_members_equal_their_own_rollouts(lattice, storage):
                 assert torch.equal(o[key], r[key]), (cfg, i, key)
 
 
+@pytest.mark.parametrize("storage", ["f32", "bf16"])
+def test_uniform_class_ensemble_equals_own_rollouts(storage):
+    """Members that all share one face / force form run the compile-time
+    specialised batched kernel."""
+    from maddening_b200.batched import LBMEnsemble, uneven_ensemble
+    nodes, bis = uneven_ensemble(5, seed=3, lo=8, hi=40, storage=storage, device="cuda")
+    states = [n.initial_state() for n in nodes]
+    ref = [n.run(s, b, 6) for n, s, b in zip(nodes, states, bis)]
+    ens = LBMEnsemble(nodes)
+    for cfg in CONFIGS[:3]:
+        out = ens.run(states, bis, 6, cfg)
+        for i, (o, r) in enumerate(zip(out, ref)):
+            for key in ("f", "density", "velocity", "pressure"):
+                assert torch.equal(o[key], r[key]), (cfg, i, key)
+
+
 def test_grouped_launch_rejects_round_robin_order():
     from maddening_b200 import _lib
     from maddening_b200.batched import LBMEnsemble

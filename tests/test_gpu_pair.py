@@ -2,7 +2,8 @@
 accesses, shuffles for the pull along the contiguous axis): bit-identical to
 the one-cell step for every storage form, lattice, face axis and force mode,
 including the periodic wrap at both ends of a row and every warp/block width
-(contiguous extents 64, 128, 192, 256)."""
+(contiguous extents 64, 128, 192, 256).  Rows that are not a multiple of 64
+cells fall back to the one-cell step."""
 
 import numpy as np
 import pytest
@@ -48,7 +49,10 @@ def _node(shape, storage, lattice, kind, cpt, seed=0):
 
 @pytest.mark.parametrize("shape,lattice", [((6, 5, 64), "D3Q19"), ((4, 3, 256), "D3Q19"),
                                            ((3, 4, 128), "D3Q19"), ((5, 2, 192), "D3Q19"),
-                                           ((1, 1, 64), "D3Q19"), ((40, 128), "D2Q9")])
+                                           ((1, 1, 64), "D3Q19"), ((40, 128), "D2Q9"),
+                                           # not row-paired: one-cell fallback
+                                           ((5, 6, 37), "D3Q19"), ((3, 4, 100), "D3Q19"),
+                                           ((33, 19), "D2Q9")])
 @pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
 @pytest.mark.parametrize("kind", ["force", "faces", "faces_contiguous", "pressure"])
 def test_paired_equals_single(shape, lattice, storage, kind):
