@@ -48,6 +48,14 @@ GRID = (256, 256, 256)
 TAU = 0.6
 U_IN = (0.05, 0.0, 0.0)
 BYTES_PER_CELL = 152  # D3Q19 FP32: 19 x 4 B read + 19 x 4 B written
+# DRAM bytes of one state step launch (k_step<19, float>) of the 256^3 FP32
+# workload, from one capture of
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:k_step -s 5 -c 3 python bench.py --steps 20 --warmup 3
+#       --no-cpu-baseline --no-variants
+# (one pass): 1.29 GB read + 1.22 GB written per launch, against 2.55 GB
+# algorithmic (the remainder of the writes is still in L2 when the launch ends).
+NCU_TRAFFIC_256_F32 = 2.51e9
 METRIC = "MLUPS (D3Q19 FP32 lattice updates/s) & HBM roofline fraction"
 WORKLOAD = "256^3 D3Q19 obstacle flow, velocity inlet + zero-gradient outlet, tau 0.6"
 
@@ -322,7 +330,11 @@ def run_ours(args):
                        "l2": "state 2 x 1.27 GB > 126 MB L2; no flush needed"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "peak_source": peak_kind, "traffic": None,
+                         "peak_source": peak_kind,
+                         "traffic": (NCU_TRAFFIC_256_F32 if GRID == (256, 256, 256)
+                                     and args.storage == "f32" else None),
+                         "traffic_unit": "DRAM bytes per launch (ncu)",
+                         "algorithmic_bytes_per_launch": bytes_per_cell * cells,
                          "bytes_per_cell": bytes_per_cell,
                          "kernel": "k_step<19,float,0,true,false> (fused pull-stream-collide, "
                                    "faces on)"},
@@ -402,35 +414,45 @@ def precision_cost(dev, steps):
 def batched_cost(dev, steps=500):
     """64 uneven D3Q19 lattices (extents log-uniform in [32, 160], tau in
     [0.55, 1.5], z walls, g_x in [1e-7, 1e-5]), 500 steps: one autotuned batched
-    launch per step against one plain rollout per instance."""
+    launch per step (FP32 and FP16 storage) against one plain rollout per
+    instance (FP32 storage, and FP16 for reference)."""
     import torch
     from maddening_b200.batched import LBMEnsemble, uneven_ensemble
-    nodes, bis = uneven_ensemble(64, seed=0, device=dev)
-    states = [n.initial_state() for n in nodes]
-    ens = LBMEnsemble(nodes)
-    cfg = ens.autotune(states, bis, n_steps=10, use_cache=False)
-    ws = torch.empty(ens.workspace_bytes(), dtype=torch.uint8, device=dev)
-    ens.run(states, bis, 3, workspace=ws)
-    for n, st, bi in zip(nodes, states, bis):
-        n.run(st, bi, 3)
-    torch.cuda.synchronize()
-    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    e[0].record()
-    ens.run(states, bis, steps, workspace=ws)
-    e[1].record()
-    e[2].record()
-    for n, st, bi in zip(nodes, states, bis):
-        n.run(st, bi, steps)
-    e[3].record()
-    torch.cuda.synchronize()
-    cells = ens.cells
-    t_b = e[0].elapsed_time(e[1]) / 1e3
-    t_p = e[2].elapsed_time(e[3]) / 1e3
-    mb, mp = cells * steps / t_b / 1e6, cells * steps / t_p / 1e6
-    return {"workload": "64 uneven D3Q19 lattices, 500 steps", "cells": cells,
-            "batched_mlups": round(mb, 1), "plain_per_instance_mlups": round(mp, 1),
-            "batched_over_plain": round(mb / mp, 3), "config": cfg,
-            "hbm_frac_batched": round(mb * 1e6 * 152 / 1e9 / _peaks()[0], 4)}
+    out = {"workload": "64 uneven D3Q19 lattices, 500 steps"}
+    for storage in ("f32", "f16"):
+        nodes, bis = uneven_ensemble(64, seed=0, storage=storage, device=dev)
+        states = [n.initial_state() for n in nodes]
+        ens = LBMEnsemble(nodes)
+        cfg = ens.autotune(states, bis, n_steps=10, use_cache=False)
+        ws = torch.empty(ens.workspace_bytes(), dtype=torch.uint8, device=dev)
+        ens.run(states, bis, 3, workspace=ws)
+        for n, st, bi in zip(nodes, states, bis):
+            n.run(st, bi, 3)
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record()
+        ens.run(states, bis, steps, workspace=ws)
+        e[1].record()
+        e[2].record()
+        for n, st, bi in zip(nodes, states, bis):
+            n.run(st, bi, steps)
+        e[3].record()
+        torch.cuda.synchronize()
+        cells = ens.cells
+        t_b = e[0].elapsed_time(e[1]) / 1e3
+        t_p = e[2].elapsed_time(e[3]) / 1e3
+        out["cells"] = cells
+        out[f"batched_{storage}_mlups"] = round(cells * steps / t_b / 1e6, 1)
+        out[f"plain_{storage}_per_instance_mlups"] = round(cells * steps / t_p / 1e6, 1)
+        out[f"config_{storage}"] = cfg
+        del ens, states, ws, nodes
+        torch.cuda.empty_cache()
+    ref = out["plain_f32_per_instance_mlups"]
+    out["batched_f32_over_plain_f32"] = round(out["batched_f32_mlups"] / ref, 3)
+    out["batched_f16_over_plain_f32"] = round(out["batched_f16_mlups"] / ref, 3)
+    out["hbm_frac_batched_f32"] = round(out["batched_f32_mlups"] * 1e6 * 152 / 1e9 / _peaks()[0], 4)
+    out["hbm_frac_batched_f16"] = round(out["batched_f16_mlups"] * 1e6 * 76 / 1e9 / _peaks()[0], 4)
+    return out
 
 
 def adjoint_cost(dev):

@@ -89,7 +89,7 @@ typedef struct {
 #define LBM_PLAN_SINGLE_CELLS 2u /* rollout steps update one cell per thread
                                    (the paired two-cell step is otherwise used
                                    for FP16/BF16 storage when the contiguous
-                                   extent is a multiple of 64) */
+                                   extent is even) */
 #define LBM_PLAN_PAIRED_CELLS 4u /* also use the paired two-cell step for FP32
                                    storage (same conditions) */
 
@@ -154,6 +154,21 @@ int lbm_update(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
                void* f_out, const lbm_step_args* args, const lbm_moments* out,
                void* workspace, size_t workspace_bytes);
 
+/* The halo-padded step, LBMNode.update_padded (lbm.py:747-897), used under
+ * spatial sharding: the plan's shape is the PADDED block, one halo cell on each
+ * side of every spatial axis (extents >= 3).  The whole block is collided, the
+ * interior is streamed across the halo without wrapping (lbm.py:270-304), the
+ * wall swap (args->wall is the padded mask) and the faces act on the interior
+ * (face planes one cell inside the block), and the interior moments are
+ * written; halo cells of f_out_pad are copied from f_pad and halo entries of
+ * the moment buffers are left untouched (the reference keeps the input's halo
+ * values).  A body-force field is padded too (the node zero-pads an
+ * interior-shaped field, as lbm.py:826-832 does).  Workspace: one population
+ * copy (lbm_state_bytes). */
+int lbm_update_padded(const lbm_plan* plan, lbm_stream_t stream, const void* f_pad,
+                      void* f_out_pad, const lbm_step_args* args, const lbm_moments* out,
+                      void* workspace, size_t workspace_bytes);
+
 /* n_steps >= 1 successive reference steps with the same inputs (the loop body
  * of GraphManager.run_scan, graph_manager.py:2697-2751).  Between steps the
  * populations stay on the device as offsets in the plan's storage form; the
@@ -203,7 +218,10 @@ typedef struct lbm_batch lbm_batch;
 typedef struct {
   int32_t blocks_per_sm; /* persistent grid = blocks_per_sm x SMs; 0 = one block per tile */
   int32_t tile_order;    /* 0: instance after instance; 1: round-robin across instances;
-                            2: instance after instance, smallest first               */
+                            2: instance after instance, smallest first.  In orders 0
+                            and 2 the members whose state steps run paired (FP16/BF16
+                            storage, even contiguous extent) come first and step
+                            with the paired kernel                                  */
   int32_t use_graph;     /* 1: record the step sequence as a CUDA graph and replay it */
   int32_t group_mib;     /* 0: every launch covers all instances.  > 0: consecutive
                             instances of the tile order (0 or 2) whose two population

@@ -76,6 +76,8 @@ _SIGS = {
                      C.POINTER(lbm_moments), _P, C.c_size_t], C.c_int),
     "lbm_update_noalloc": ([_P, _P, _P, _P, C.POINTER(lbm_step_args),
                             C.POINTER(lbm_moments)], C.c_int),
+    "lbm_update_padded": ([_P, _P, _P, _P, C.POINTER(lbm_step_args), C.POINTER(lbm_moments),
+                           _P, C.c_size_t], C.c_int),
     "lbm_adjoint_workspace_bytes": ([_P, C.c_int64, C.c_int64, C.POINTER(C.c_size_t)],
                                     C.c_int),
     "lbm_rollout_forward": ([_P, _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(lbm_step_args),

@@ -234,8 +234,9 @@ int launch_staged(const lbm::StepArgs& a, cudaStream_t s) {
 
 // Paired-cell state step (lbm_pair.cuh): the default for 16-bit storage,
 // opt-in for FP32 (LBM_PLAN_PAIRED_CELLS), off with LBM_PLAN_SINGLE_CELLS.
-// Rows must split into whole warp segments of 64 cells; state planes and the
-// wall mask must be aligned for the pair width.
+// Rows of even length (row segments when they split into warps of 64 cells,
+// instance-wide pairs otherwise); state planes and the wall mask aligned for
+// the pair width.
 template <class S>
 bool pair_ok(const lbm_plan* p, const lbm::StepArgs& a) {
   if constexpr (sizeof(S) == 8) {
@@ -244,7 +245,7 @@ bool pair_ok(const lbm_plan* p, const lbm::StepArgs& a) {
     if (p->flags & LBM_PLAN_SINGLE_CELLS) return false;
     if (sizeof(S) == 4 && !(p->flags & LBM_PLAN_PAIRED_CELLS)) return false;
     const uintptr_t al = 2 * sizeof(S);
-    return p->g.n2 % 64 == 0 && reinterpret_cast<uintptr_t>(a.pin) % al == 0 &&
+    return p->g.n2 % 2 == 0 && reinterpret_cast<uintptr_t>(a.pin) % al == 0 &&
            reinterpret_cast<uintptr_t>(a.pout) % al == 0 &&
            reinterpret_cast<uintptr_t>(a.wall) % 2 == 0;
   }
@@ -265,13 +266,28 @@ void launch_pair_w(const lbm::StepArgs& a, cudaStream_t s) {
 }
 
 template <int Q, class S>
+void launch_gpair(const lbm::StepArgs& a, cudaStream_t s) {
+  const unsigned grid = grid_for(a.g.ncell / 2);
+  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (faces) {
+    if (force) lbm::k_step_gpair<Q, S, true, true><<<grid, lbm::kBlock, 0, s>>>(a);
+    else lbm::k_step_gpair<Q, S, true, false><<<grid, lbm::kBlock, 0, s>>>(a);
+  } else {
+    if (force) lbm::k_step_gpair<Q, S, false, true><<<grid, lbm::kBlock, 0, s>>>(a);
+    else lbm::k_step_gpair<Q, S, false, false><<<grid, lbm::kBlock, 0, s>>>(a);
+  }
+}
+
+template <int Q, class S>
 int launch_pair(const lbm::StepArgs& a, cudaStream_t s) {
   if constexpr (sizeof(S) == 8) {
     return fail(LBM_ERR_UNSUPPORTED, "paired step has no FP64 form");
   } else {
     if (a.g.n2 % 256 == 0) launch_pair_w<Q, S, 4>(a, s);
     else if (a.g.n2 % 128 == 0) launch_pair_w<Q, S, 2>(a, s);
-    else launch_pair_w<Q, S, 1>(a, s);
+    else if (a.g.n2 % 64 == 0) launch_pair_w<Q, S, 1>(a, s);
+    else launch_gpair<Q, S>(a, s);
     return cuda_check(cudaGetLastError(), "k_step_pair launch");
   }
 }
@@ -281,6 +297,38 @@ template <int Q, class S>
 int launch_state_step(const lbm_plan* p, const lbm::StepArgs& m, cudaStream_t s) {
   if (pair_ok<S>(p, m)) return launch_pair<Q, S>(m, s);
   return launch_step<Q, S>(m, false, s);
+}
+
+template <int Q, class S>
+int launch_step_padded(const lbm::StepArgs& a, cudaStream_t s) {
+  const unsigned grid = grid_for(a.g.ncell);
+  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (faces) {
+    if (force) lbm::k_step_padded<Q, S, true, true><<<grid, lbm::kBlock, 0, s>>>(a);
+    else lbm::k_step_padded<Q, S, true, false><<<grid, lbm::kBlock, 0, s>>>(a);
+  } else {
+    if (force) lbm::k_step_padded<Q, S, false, true><<<grid, lbm::kBlock, 0, s>>>(a);
+    else lbm::k_step_padded<Q, S, false, false><<<grid, lbm::kBlock, 0, s>>>(a);
+  }
+  return cuda_check(cudaGetLastError(), "k_step_padded launch");
+}
+
+// Collide the whole padded block into the workspace, then the padded step.
+template <int Q, class S>
+int run_padded(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in,
+               void* f_out, char* ws) {
+  (void)p;
+  lbm::StepArgs m = a;
+  m.rho = m.vel = m.prs = nullptr;  // halo moments stay the caller's
+  m.f_in = f_in;
+  m.pout = ws;
+  int rc = launch_prepare<Q, S>(m, s);
+  if (rc) return rc;
+  a.pin = ws;
+  a.f_in = f_in;
+  a.f_out = f_out;
+  return launch_step_padded<Q, S>(a, s);
 }
 
 template <int Q, class S>
@@ -550,31 +598,39 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
 // ---------------------------------------------------------------------------
 
 // A contiguous range [t0, t1) of the tile list whose instances are stepped
-// together; grid = blocks of the persistent launch for that range.
+// together; grid = blocks of the persistent launch for that range; pair = its
+// state steps run the paired kernel (16-bit storage, even rows).
 struct TileRange {
   uint32_t t0, t1;
   unsigned grid;
+  bool pair;
 };
 
 // Prepare pass over all tiles, then for each instance group its n - 1 state
 // steps and its last step.  A group whose two population copies fit in L2
 // stays there for all of its steps.
 template <int Q, class S, int MODE, int SPEC>
-void batched_launch(const lbm::StepArgs* args, const lbm::BatchTile* t, uint32_t nt, unsigned grid,
-                    int which, cudaStream_t s) {
+void batched_launch(bool pair, const lbm::StepArgs* args, const lbm::BatchTile* t, uint32_t nt,
+                    unsigned grid, int which, cudaStream_t s) {
+  if constexpr (MODE == lbm::kOutState && sizeof(S) == 2) {
+    if (pair) {
+      lbm::k_batched_pair<Q, S, SPEC><<<grid, lbm::kBlock, 0, s>>>(args, t, nt, which);
+      return;
+    }
+  }
   lbm::k_batched_step<Q, S, MODE, SPEC><<<grid, lbm::kBlock, 0, s>>>(args, t, nt, which);
 }
 
 // spec: 0 = per-tile run-time choice, else 1 + 2 FACES + FORCE shared by all members
 template <int Q, class S, int MODE>
-void batched_step(int spec, const lbm::StepArgs* args, const lbm::BatchTile* t, uint32_t nt,
-                  unsigned grid, int which, cudaStream_t s) {
+void batched_step(int spec, bool pair, const lbm::StepArgs* args, const lbm::BatchTile* t,
+                  uint32_t nt, unsigned grid, int which, cudaStream_t s) {
   switch (spec) {
-    case 1: batched_launch<Q, S, MODE, 1>(args, t, nt, grid, which, s); break;
-    case 2: batched_launch<Q, S, MODE, 2>(args, t, nt, grid, which, s); break;
-    case 3: batched_launch<Q, S, MODE, 3>(args, t, nt, grid, which, s); break;
-    case 4: batched_launch<Q, S, MODE, 4>(args, t, nt, grid, which, s); break;
-    default: batched_launch<Q, S, MODE, 0>(args, t, nt, grid, which, s); break;
+    case 1: batched_launch<Q, S, MODE, 1>(pair, args, t, nt, grid, which, s); break;
+    case 2: batched_launch<Q, S, MODE, 2>(pair, args, t, nt, grid, which, s); break;
+    case 3: batched_launch<Q, S, MODE, 3>(pair, args, t, nt, grid, which, s); break;
+    case 4: batched_launch<Q, S, MODE, 4>(pair, args, t, nt, grid, which, s); break;
+    default: batched_launch<Q, S, MODE, 0>(pair, args, t, nt, grid, which, s); break;
   }
 }
 
@@ -600,8 +656,9 @@ int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t
     const lbm::BatchTile* t = tiles + r.t0;
     const uint32_t nt = r.t1 - r.t0;
     for (int64_t k = 1; k < n; ++k)
-      batched_step<Q, S, lbm::kOutState>(spec, args, t, nt, r.grid, static_cast<int>(k % 2), ls);
-    batched_step<Q, S, lbm::kOutAoS>(spec, args, t, nt, r.grid, 2, ls);
+      batched_step<Q, S, lbm::kOutState>(spec, r.pair, args, t, nt, r.grid,
+                                         static_cast<int>(k % 2), ls);
+    batched_step<Q, S, lbm::kOutAoS>(spec, false, args, t, nt, r.grid, 2, ls);
   }
   rc = cuda_check(cudaGetLastError(), "k_batched_step launch");
   if (use_graph) {
@@ -630,9 +687,11 @@ struct lbm_batch {
   // [0] instance-major in member order, [1] round-robin across members,
   // [2] instance-major from the smallest member to the largest
   std::vector<lbm::BatchTile> tiles[kTileOrders];
-  // members in the order of tile lists 0 and 2, with their first tile
+  // members in the order of tile lists 0 and 2 (members whose state steps can
+  // run paired -- 16-bit storage, even rows -- first), with their first tile
   std::vector<int> order[kTileOrders];
   std::vector<uint32_t> first_tile[kTileOrders];
+  int npair = 0;  // number of those members
   cudaStream_t side = nullptr;
 };
 
@@ -794,6 +853,48 @@ int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, voi
                   n_steps > 1 ? 2 : 1);
 }
 
+int lbm_update_padded(const lbm_plan* p, lbm_stream_t stream, const void* f_pad,
+                      void* f_out_pad, const lbm_step_args* args, const lbm_moments* out,
+                      void* workspace, size_t workspace_bytes) {
+  if (p == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
+  if (f_pad == nullptr || f_out_pad == nullptr) return fail(LBM_ERR_INVALID, "f is NULL");
+  for (int d = 0; d < p->D; ++d)
+    if (p->shape[d] < 3)
+      return fail(LBM_ERR_INVALID,
+                  "padded extent %lld along axis %d: one halo cell per side needs >= 3",
+                  (long long)p->shape[d], d);
+  const size_t need = state_bytes(p);
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", need,
+                workspace_bytes);
+  lbm::StepArgs a;
+  int rc = build_args(p, args, out, &a);
+  if (rc) return rc;
+  a.face_inset = 1;
+  if (a.face[1].kind == lbm::kFaceZeroGrad && p->shape[a.face[1].ref_axis] < 5)
+    return fail(LBM_ERR_INVALID,
+                "zero-gradient face needs >= 3 interior cells along axis %d",
+                a.face[1].ref_axis);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  if (p->Q == 19) {
+    switch (p->storage) {
+      case LBM_STORE_F32: return run_padded<19, float>(p, s, a, f_pad, f_out_pad, ws);
+      case LBM_STORE_F16: return run_padded<19, __half>(p, s, a, f_pad, f_out_pad, ws);
+      case LBM_STORE_BF16: return run_padded<19, __nv_bfloat16>(p, s, a, f_pad, f_out_pad, ws);
+      case LBM_STORE_F64: return run_padded<19, double>(p, s, a, f_pad, f_out_pad, ws);
+    }
+  } else {
+    switch (p->storage) {
+      case LBM_STORE_F32: return run_padded<9, float>(p, s, a, f_pad, f_out_pad, ws);
+      case LBM_STORE_F16: return run_padded<9, __half>(p, s, a, f_pad, f_out_pad, ws);
+      case LBM_STORE_BF16: return run_padded<9, __nv_bfloat16>(p, s, a, f_pad, f_out_pad, ws);
+      case LBM_STORE_F64: return run_padded<9, double>(p, s, a, f_pad, f_out_pad, ws);
+    }
+  }
+  return fail(LBM_ERR_INVALID, "bad storage");
+}
+
 int lbm_update_noalloc(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
                        void* f_out, const lbm_step_args* args, const lbm_moments* out) {
   if (plan == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
@@ -901,13 +1002,20 @@ int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
     delete b;
     return fail(LBM_ERR_INVALID, "ensemble too large");
   }
-  std::vector<int> by_size(n);
-  for (int i = 0; i < n; ++i) by_size[i] = i;
+  auto pairable = [&](int i) {
+    return (b->storage == LBM_STORE_F16 || b->storage == LBM_STORE_BF16) &&
+           plans[i]->g.n2 % 2 == 0 && !(plans[i]->flags & LBM_PLAN_SINGLE_CELLS);
+  };
+  std::vector<int> by_member(n), by_size(n);
+  for (int i = 0; i < n; ++i) by_member[i] = by_size[i] = i;
   std::stable_sort(by_size.begin(), by_size.end(),
                    [&](int x, int y) { return plans[x]->g.ncell < plans[y]->g.ncell; });
+  for (auto* v : {&by_member, &by_size})
+    std::stable_partition(v->begin(), v->end(), pairable);
+  for (int i = 0; i < n; ++i) b->npair += pairable(i) ? 1 : 0;
   for (int k : {0, 2}) {
     for (int j = 0; j < n; ++j) {
-      const int i = k == 0 ? j : by_size[j];
+      const int i = k == 0 ? by_member[j] : by_size[j];
       b->order[k].push_back(i);
       b->first_tile[k].push_back(static_cast<uint32_t>(b->tiles[k].size()));
       b->tiles[k].insert(b->tiles[k].end(), per[i].begin(), per[i].end());
@@ -1018,25 +1126,38 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
   // Instance groups: consecutive members of the tile order whose two
   // population copies together stay within group_mib (a member larger than
   // that is a group of its own); 0 = all members in every launch.
+  // Members whose state steps run paired come first in tile orders 0 and 2;
+  // their wall masks must be 2-byte aligned (else nothing runs paired).
+  int npair = c.tile_order == 1 ? 0 : b->npair;
+  for (int j = 0; j < npair; ++j) {
+    const int i = b->order[c.tile_order][j];
+    if (reinterpret_cast<uintptr_t>(args[i].wall) % 2 != 0) npair = 0;
+  }
   std::vector<TileRange> groups;
+  const auto& ord = b->order[c.tile_order];
+  const auto& ft = b->first_tile[c.tile_order];
+  const uint32_t tsplit = npair > 0 && npair < b->n ? ft[npair] : (npair > 0 ? ntiles : 0u);
+  auto add_range = [&](uint32_t t0, uint32_t t1, bool pair) {
+    if (t1 > t0) groups.push_back(TileRange{t0, t1, grid_for_tiles(t1 - t0), pair});
+  };
   if (c.group_mib == 0) {
-    groups.push_back(TileRange{0, ntiles, grid_for_tiles(ntiles)});
+    add_range(0, tsplit, true);
+    add_range(tsplit, ntiles, false);
   } else {
     const size_t budget = static_cast<size_t>(c.group_mib) << 20;
-    const auto& ord = b->order[c.tile_order];
-    const auto& ft = b->first_tile[c.tile_order];
     size_t used = 0;
     uint32_t t0 = 0;
     for (size_t j = 0; j < ord.size(); ++j) {
       const size_t need = 2 * align256(state_bytes(b->plans[ord[j]]));
-      if (j > 0 && used + need > budget) {
-        groups.push_back(TileRange{t0, ft[j], grid_for_tiles(ft[j] - t0)});
+      const bool split = static_cast<int>(j) == npair;  // pair / one-cell boundary
+      if (j > 0 && (used + need > budget || split)) {
+        add_range(t0, ft[j], static_cast<int>(j) <= npair);
         t0 = ft[j];
         used = 0;
       }
       used += need;
     }
-    groups.push_back(TileRange{t0, ntiles, grid_for_tiles(ntiles - t0)});
+    add_range(t0, ntiles, static_cast<int>(ord.size()) <= npair);
   }
   const unsigned grid_all = grid_for_tiles(ntiles);
   const bool g = c.use_graph != 0;

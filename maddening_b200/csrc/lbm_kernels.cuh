@@ -125,6 +125,9 @@ struct StepArgs {
   void* prs;
   uint32_t mflags;
   int* status;  // device word; bit 0 set when a bounded wait gave up (staged path)
+  // Face planes sit this many cells inside the lattice: 0, or 1 for a
+  // halo-padded block (the faces act on the interior).
+  uint32_t face_inset;
 };
 
 constexpr uint32_t kMomDensityDev = 1u;
@@ -540,7 +543,7 @@ __device__ __forceinline__ void apply_faces(const StepArgs& a, const Cell& x,
     if (fc.kind == kFaceNone) continue;
     const uint32_t coord = fc.axis == 0 ? x.i0 : (fc.axis == 1 ? x.i1 : x.k);
     const uint32_t nax = fc.axis == 0 ? g.n0 : (fc.axis == 1 ? g.n1 : g.n2);
-    if (coord != (fc.side == 0 ? 0u : nax - 1)) continue;
+    if (coord != (fc.side == 0 ? a.face_inset : nax - 1 - a.face_inset)) continue;
     if (fc.kind == kFacePressure) face_pressure<Q, R>(d, a, fi);
     else if (fc.kind == kFaceVelocity) face_velocity<Q, R>(d, a, fi);
     else face_zero_gradient<Q, S>(d, a, fi, x.i0, x.i1, x.k);
@@ -638,12 +641,46 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
   if (cidx < a.g.ncell) step_cell<Q, S, MODE, FACES, FORCE>(a, cidx);
 }
 
+// Halo-padded block (the reference's update_padded, lbm.py:747-897): one halo
+// cell on every side of every spatial axis.  p (the whole block collided) is
+// pulled across the halo without wrapping -- interior cells never reach past
+// the halo -- then wall swap, faces on the interior planes (face_inset = 1),
+// moments and f_bc of the interior cells are written; a halo cell keeps its
+// input populations (f_in copied to f_out) and its moment outputs untouched.
+template <int Q, class S, bool FACES, bool FORCE>
+__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+    k_step_padded(const __grid_constant__ StepArgs a) {
+  using R = typename StoreT<S>::R;
+  using IO = typename StoreT<S>::IO;
+  const Geo& g = a.g;
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= g.ncell) return;
+  const Cell x = locate(g, c);
+  const bool halo = (Lat<Q>::D == 3 && (x.i0 == 0 || x.i0 == g.n0 - 1)) || x.i1 == 0 ||
+                    x.i1 == g.n1 - 1 || x.k == 0 || x.k == g.n2 - 1;
+  if (halo) {
+    const IO* fi = static_cast<const IO*>(a.f_in) + static_cast<size_t>(c) * Q;
+    IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(c) * Q;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) fo[q] = fi[q];
+    return;
+  }
+  R d[Q];
+  pull_cell<Q, S>(a, x, d);
+  finish_cell<Q, S, kOutAoS, FACES, FORCE>(a, x, d);
+}
+
 // ---------------------------------------------------------------------------
 // Batched ensemble: many lattices (own shape, tau, force, walls) in one launch
 // ---------------------------------------------------------------------------
 
-// A tile is kBatchTile consecutive cells of one instance.
-constexpr int kBatchTile = 2 * kBlock;
+// A tile is kBatchTile consecutive cells of one instance (a multiple of
+// 2 kBlock: the paired kernel gives each thread kBatchTile / (2 kBlock) pairs).
+#ifndef LBM_BATCH_TILE
+#define LBM_BATCH_TILE (2 * LBM_STEP_BLOCK)
+#endif
+constexpr int kBatchTile = LBM_BATCH_TILE;
+static_assert(kBatchTile % (2 * kBlock) == 0, "batch tiles hold whole pair rows of a block");
 struct BatchTile {
   uint32_t inst;
   uint32_t first;
@@ -720,7 +757,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
       cur = tile.inst;
     }
 #pragma unroll 1
-    for (int j = 0; j < 2; ++j) {
+    for (int j = 0; j < kBatchTile / kBlock; ++j) {
       const uint32_t c = tile.first + j * kBlock + threadIdx.x;
       if (c < sa.g.ncell) {
         if (sa.force_mode != 0) prepare_cell<Q, S, true>(sa, c);

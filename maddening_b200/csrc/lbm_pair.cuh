@@ -25,9 +25,14 @@
 // bit-identical; the wall swap is skipped by warps without a wall cell and the
 // face checks by pairs that cannot touch a face.
 //
-// Requirements (checked on the host): n2 a multiple of 64 W, state planes and
-// the wall mask aligned for the pair width.  Used for the state-to-state steps
-// of a rollout; the other modes keep the one-cell kernels.
+// A second form (k_step_gpair) takes any even row length: pairs follow the
+// instance-wide cell index, each lane finds its own row, and the lanes whose
+// neighbour pair lies in another row or outside the warp load it themselves.
+//
+// Requirements (checked on the host): an even contiguous extent n2 (a multiple
+// of 64 W for the row-segment form), state planes and the wall mask aligned for
+// the pair width.  Used for the state-to-state steps of a rollout; the other
+// modes keep the one-cell kernels.
 #pragma once
 
 #include "lbm_kernels.cuh"
@@ -112,6 +117,87 @@ __device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, floa
   collide<Q, float, FORCE>(d, m, F, static_cast<float>(a.omega), static_cast<float>(a.guo_c));
 }
 
+// Everything after the plane loads of one thread's pair (k, k+1) of row
+// `rbase`: lane l's own pair words v[q]; e[q] the word of the pair before
+// (c2 > 0, lanes with edge_prev) or after (c2 < 0, lanes with edge_next) for
+// the lanes whose neighbour pair is not held by the adjacent lane.  All 32
+// lanes of the warp must call it (shuffles, vote); `store` = false for lanes
+// that only pad the warp.
+template <int Q, class S, bool FACES, bool FORCE>
+__device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint32_t i1,
+                                            uint32_t k, uint32_t rbase, bool edge_prev,
+                                            bool edge_next, const typename PairT<S>::P (&v)[Q],
+                                            const typename PairT<S>::P (&e)[Q], bool store) {
+  using PT = PairT<S>;
+  using P = typename PT::P;
+  const Geo& g = a.g;
+  float da[Q], db[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c2 = Lat<Q>::c2(q);
+    if (c2 == 0) {
+      da[q] = PT::lo(v[q]);
+      db[q] = PT::hi(v[q]);
+    } else if (c2 > 0) {
+      P nb = PT::shup(v[q]);
+      if (edge_prev) nb = e[q];
+      da[q] = PT::hi(nb);
+      db[q] = PT::lo(v[q]);
+    } else {
+      P nb = PT::shdn(v[q]);
+      if (edge_next) nb = e[q];
+      da[q] = PT::hi(v[q]);
+      db[q] = PT::lo(nb);
+    }
+  }
+  bool wa = false, wb = false;
+  if (a.wall != nullptr) {
+    const uint32_t w2 = __ldg(reinterpret_cast<const unsigned short*>(a.wall + rbase + k));
+    wa = (w2 & 0xffu) != 0;
+    wb = (w2 >> 8) != 0;
+  }
+  Cell xa, xb;
+  xa.c = rbase + k;
+  xa.i0 = i0;
+  xa.i1 = i1;
+  xa.k = k;
+  xa.row = rbase;
+  xb = xa;
+  xb.c = xa.c + 1;
+  xb.k = k + 1;
+  // Wall swap only in warps that hold a wall cell (obstacles are clustered).
+  if (__any_sync(0xffffffffu, wa || wb)) {
+    if (wa) wall_swap<Q>(da);
+    if (wb) wall_swap<Q>(db);
+  }
+  if constexpr (FACES) {
+    // Only pairs on a face plane run the face code: rows on faces of axes 0
+    // and 1, the first and the last pair of a row on faces of the contiguous axis.
+    bool near = false;
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+      const FaceK& fc = a.face[fi];
+      if (fc.kind == kFaceNone) continue;
+      const uint32_t ins = a.face_inset;
+      if (fc.axis == 0) near |= i0 == (fc.side == 0 ? ins : g.n0 - 1 - ins);
+      else if (fc.axis == 1) near |= i1 == (fc.side == 0 ? ins : g.n1 - 1 - ins);
+      else near |= (fc.side == 0 ? ins : g.n2 - 1 - ins) - k <= 1u;  // k or k + 1
+    }
+    if (near) {
+      if (!wa) apply_faces<Q, S>(a, xa, da);
+      if (!wb) apply_faces<Q, S>(a, xb, db);
+    }
+  }
+  pair_cell<Q, S, FORCE>(a, xa, da);
+  pair_cell<Q, S, FORCE>(a, xb, db);
+  if (!store) return;
+  S* pout = static_cast<S*>(a.pout);
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+    PT::st(pout + (static_cast<uint32_t>(q) * g.ncell + rbase + k), da[q], db[q]);
+}
+
+// Row-segment form: rows of 64 W cells or a multiple (see the header comment).
 template <int Q, class S, bool FACES, bool FORCE, int W>
 __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
     k_step_pair(const __grid_constant__ StepArgs a) {
@@ -144,69 +230,93 @@ __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
     if (c2 > 0 && lane == 0) e[q] = PT::ld(base + kprev);
     if (c2 < 0 && lane == 31) e[q] = PT::ld(base + knext);
   }
-  float da[Q], db[Q];
+  pair_finish<Q, S, FACES, FORCE>(a, i0, i1, k, row * g.n2, lane == 0, lane == 31, v, e, true);
+}
+
+// Pairs of one instance-wide index: pair j holds cells 2j, 2j + 1 (rows of even
+// length, so a pair never spans two rows).  Row coordinates and source rows
+// are per lane; a lane whose neighbour pair lies in another row (k = 0 or
+// k + 2 = n2) or outside the warp loads it itself.
+template <int Q, class S, bool FACES, bool FORCE>
+__device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
+  using PT = PairT<S>;
+  using P = typename PT::P;
+  const Geo& g = a.g;
+  const uint32_t npairs = g.ncell >> 1;
+  const bool valid = pidx < npairs;
+  const Cell x = locate(g, 2u * (valid ? pidx : npairs - 1u));
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
+  const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
+  const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.n2 : 0u - g.n2;  // i1 - 1
+  const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.n2 : g.n2;
+  const bool edge_prev = lane == 0 || x.k == 0;
+  const bool edge_next = lane == 31 || x.k + 2 == g.n2;
+  const uint32_t kprev = (x.k == 0 ? g.n2 : x.k) - 2u;
+  const uint32_t knext = x.k + 2 == g.n2 ? 0u : x.k + 2;
+  const S* pin = static_cast<const S*>(a.pin);
+  P v[Q];
+  P e[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    const int c2 = Lat<Q>::c2(q);
-    if (c2 == 0) {
-      da[q] = PT::lo(v[q]);
-      db[q] = PT::hi(v[q]);
-    } else if (c2 > 0) {
-      P nb = PT::shup(v[q]);
-      if (lane == 0) nb = e[q];
-      da[q] = PT::hi(nb);
-      db[q] = PT::lo(v[q]);
-    } else {
-      P nb = PT::shdn(v[q]);
-      if (lane == 31) nb = e[q];
-      da[q] = PT::hi(v[q]);
-      db[q] = PT::lo(nb);
+    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
+    uint32_t off = x.row;
+    if (c0 > 0) off += dm0;
+    if (c0 < 0) off += dp0;
+    if (c1 > 0) off += dm1;
+    if (c1 < 0) off += dp1;
+    const S* base = pin + (static_cast<uint32_t>(q) * g.ncell + off);
+    v[q] = PT::ld(base + x.k);
+    if (c2 > 0 && edge_prev) e[q] = PT::ld(base + kprev);
+    if (c2 < 0 && edge_next) e[q] = PT::ld(base + knext);
+  }
+  pair_finish<Q, S, FACES, FORCE>(a, x.i0, x.i1, x.k, x.row, edge_prev, edge_next, v, e, valid);
+}
+
+template <int Q, class S, bool FACES, bool FORCE>
+__global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
+    k_step_gpair(const __grid_constant__ StepArgs a) {
+  gpair_step<Q, S, FACES, FORCE>(a, blockIdx.x * kBlock + threadIdx.x);
+}
+
+// Batched ensemble, state steps of members with even rows: a tile of
+// kBatchTile cells is kBatchTile / 2 pairs, kBatchTile / (2 kBlock) per thread
+// (see k_batched_step for the tile walk and SPEC).
+template <int Q, class S, int SPEC>
+__global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
+    k_batched_pair(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
+                   uint32_t ntiles, int which) {
+  __shared__ StepArgs sa;
+  uint32_t cur = 0xffffffffu;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const BatchTile tile = tiles[t];
+    if (tile.inst != cur) {
+      __syncthreads();
+      stage_args(sa, args[kBatchArgs * tile.inst + which]);
+      __syncthreads();
+      cur = tile.inst;
+    }
+#pragma unroll 1
+    for (int j = 0; j < kBatchTile / (2 * kBlock); ++j) {
+      const uint32_t pidx = (tile.first >> 1) + j * kBlock + threadIdx.x;
+      // whole warps past the member's last pair skip the step; a partial warp
+      // runs it with its extra lanes clamped
+      if ((((tile.first >> 1) + j * kBlock + (threadIdx.x & ~31u)) << 1) >= sa.g.ncell) break;
+      if constexpr (SPEC == 0) {
+        const bool faces = sa.face[0].kind != kFaceNone || sa.face[1].kind != kFaceNone;
+        const bool force = sa.force_mode != 0;
+        if (faces) {
+          if (force) gpair_step<Q, S, true, true>(sa, pidx);
+          else gpair_step<Q, S, true, false>(sa, pidx);
+        } else {
+          if (force) gpair_step<Q, S, false, true>(sa, pidx);
+          else gpair_step<Q, S, false, false>(sa, pidx);
+        }
+      } else {
+        gpair_step<Q, S, ((SPEC - 1) & 2) != 0, ((SPEC - 1) & 1) != 0>(sa, pidx);
+      }
     }
   }
-  const uint32_t rbase = row * g.n2;
-  bool wa = false, wb = false;
-  if (a.wall != nullptr) {
-    const uint32_t w2 = __ldg(reinterpret_cast<const unsigned short*>(a.wall + rbase + k));
-    wa = (w2 & 0xffu) != 0;
-    wb = (w2 >> 8) != 0;
-  }
-  Cell xa, xb;
-  xa.c = rbase + k;
-  xa.i0 = i0;
-  xa.i1 = i1;
-  xa.k = k;
-  xa.row = rbase;
-  xb = xa;
-  xb.c = xa.c + 1;
-  xb.k = k + 1;
-  // Wall swap only in warps that hold a wall cell (obstacles are clustered).
-  if (__any_sync(0xffffffffu, wa || wb)) {
-    if (wa) wall_swap<Q>(da);
-    if (wb) wall_swap<Q>(db);
-  }
-  if constexpr (FACES) {
-    // Face rows (axes 0 and 1) are block-uniform; on the contiguous axis only
-    // the first and the last pair of a row can hold a face cell.
-    bool near = false;
-#pragma unroll
-    for (int fi = 0; fi < 2; ++fi) {
-      const FaceK& fc = a.face[fi];
-      if (fc.kind == kFaceNone) continue;
-      if (fc.axis == 0) near |= i0 == (fc.side == 0 ? 0u : g.n0 - 1);
-      else if (fc.axis == 1) near |= i1 == (fc.side == 0 ? 0u : g.n1 - 1);
-      else near |= fc.side == 0 ? k == 0 : k + 2 == g.n2;
-    }
-    if (near) {
-      if (!wa) apply_faces<Q, S>(a, xa, da);
-      if (!wb) apply_faces<Q, S>(a, xb, db);
-    }
-  }
-  pair_cell<Q, S, FORCE>(a, xa, da);
-  pair_cell<Q, S, FORCE>(a, xb, db);
-  S* pout = static_cast<S*>(a.pout);
-#pragma unroll
-  for (int q = 0; q < Q; ++q)
-    PT::st(pout + (static_cast<uint32_t>(q) * g.ncell + rbase + k), da[q], db[q]);
 }
 
 }  // namespace lbm

@@ -19,8 +19,8 @@ Additions beyond the reference (documented extensions):
   arithmetic) or ``"f64"`` (FP64 throughout; state arrays are float64).
 * ``cells_per_thread`` -- kernel form of the steps inside ``run``: ``None``
   (default: two neighbouring cells per thread for FP16/BF16 storage when the
-  contiguous extent is a multiple of 64, else one), ``1`` or ``2`` (also for
-  FP32).  Every form gives bit-identical results.
+  contiguous extent is even, else one), ``1`` or ``2`` (also for FP32).  Every
+  form gives bit-identical results.
 """
 
 from __future__ import annotations
@@ -219,11 +219,17 @@ class LBMNode(SimulationNode):
         return t.contiguous()
 
     # -- boundary inputs (lbm.py:910-968) ------------------------------------
-    def _step_args(self, state: dict, bi: dict, dev):
-        """Builds the C step arguments; returns (args, keep-alive tensors)."""
+    def _step_args(self, state: dict, bi: dict, dev, shape=None, interior=None):
+        """Builds the C step arguments; returns (args, keep-alive tensors).
+
+        ``shape``: the lattice the arrays describe (default ``grid_shape``; the
+        padded block for ``update_padded``).  ``interior``: for a padded block,
+        its interior shape -- a body-force field of that shape is zero-padded
+        by one cell per side (lbm.py:826-832)."""
         a = _lib.lbm_step_args()
         keep = []
         D = self._D
+        shape = self._grid_shape if shape is None else tuple(shape)
         # wall mask precedence: wall_mask_update > state["wall_mask"] > node mask
         if "wall_mask_update" in bi:
             wall = torch.as_tensor(bi["wall_mask_update"], device=dev)
@@ -231,9 +237,8 @@ class LBMNode(SimulationNode):
             wall = torch.as_tensor(state["wall_mask"], device=dev)
         else:
             wall = self._wall_mask_on(dev)
-        if tuple(wall.shape) != self._grid_shape:
-            raise ValueError(f"wall mask shape {tuple(wall.shape)} != grid_shape "
-                             f"{self._grid_shape}")
+        if tuple(wall.shape) != shape:
+            raise ValueError(f"wall mask shape {tuple(wall.shape)} != grid_shape {shape}")
         wall = (wall != 0).to(torch.uint8).contiguous() if wall.dtype != torch.uint8 \
             else wall.contiguous()
         keep.append(wall)
@@ -259,7 +264,11 @@ class LBMNode(SimulationNode):
                         a.force[d] = float(vals[d])
                         dev_vals[6 + d] = float(vals[d])
             else:
-                field = self._as_field(ft, self._grid_shape + (D,), dev)
+                if interior is not None and tuple(ft.shape) == tuple(interior) + (D,):
+                    ft = torch.nn.functional.pad(
+                        torch.as_tensor(ft, device=dev).to(self._io_dtype).movedim(-1, 0),
+                        (1, 1) * D).movedim(0, -1)
+                field = self._as_field(ft, shape + (D,), dev)
                 keep.append(field)
                 a.force_mode = _lib.FORCE_FIELD
                 a.force_field = field.data_ptr()
@@ -366,11 +375,65 @@ class LBMNode(SimulationNode):
             raise ValueError("n_steps must be >= 1")
         return self._advance(state, boundary_inputs, int(n_steps))
 
+    def _padded_plan(self, pshape) -> _lib.Plan:
+        plans = self.__dict__.setdefault("_padded_plans", {})
+        if pshape not in plans:
+            plans[pshape] = _lib.Plan(self._Q, pshape, self._tau, self._storage)
+        return plans[pshape]
+
     def update_padded(self, state_padded, boundary_inputs, dt, *, static_padded=None,
                       shard_info=None):
-        raise NotImplementedError(
-            "LBMNode (B200) runs on one GPU; the halo-padded sharded step "
-            "(update_padded) is not provided")
+        """Halo-aware step on a block padded by one cell per side of every
+        spatial axis (lbm.py:747-897), as ``ShardedStencilNode`` calls it after
+        a halo exchange: the whole block is collided, the interior streams
+        across the halo, the wall swap and the faces act on the interior, and
+        the outputs keep the input's halo entries.  ``state_padded`` holds
+        ``f``, ``density``, ``velocity``, ``pressure`` (and ``wall_mask``) of
+        the padded block; ``body_force`` may be (D,), a padded field or an
+        interior-shaped field (zero-padded).  ``static_padded`` and
+        ``shard_info`` are accepted for the contract and unused, as in the
+        reference."""
+        del static_padded, shard_info
+        dev = self._dev()
+        f = torch.as_tensor(state_padded["f"], device=dev).to(self._io_dtype).contiguous()
+        D, Q = self._D, self._Q
+        pshape = tuple(int(n) for n in f.shape[:-1])
+        if len(pshape) != D or f.shape[-1] != Q:
+            raise ValueError(f"state_padded['f'] must have shape (*padded_grid, {Q}) with "
+                             f"{D} spatial axes; got {tuple(f.shape)}")
+        if min(pshape) < 3:
+            raise ValueError(f"padded extents {pshape}: one halo cell per side needs >= 3")
+        interior = tuple(n - 2 for n in pshape)
+        bi = boundary_inputs or {}
+        if ("wall_mask_update" not in bi and "wall_mask" not in state_padded
+                and pshape != self._grid_shape):
+            raise ValueError("update_padded needs the padded wall mask: "
+                             "state_padded['wall_mask'] or boundary_inputs['wall_mask_update']")
+        plan = self._padded_plan(pshape)
+        args, keep = self._step_args(state_padded, bi, dev, shape=pshape, interior=interior)
+
+        def padded_field(key, shape):
+            t = torch.as_tensor(state_padded[key], device=dev).to(self._io_dtype)
+            if tuple(t.shape) != shape:
+                raise ValueError(f"state_padded[{key!r}] shape {tuple(t.shape)} != {shape}")
+            return t.clone().contiguous()
+
+        rho = padded_field("density", pshape)
+        vel = padded_field("velocity", pshape + (D,))
+        prs = padded_field("pressure", pshape)
+        f_out = torch.empty_like(f)
+        m = _lib.lbm_moments()
+        m.density, m.velocity, m.pressure = rho.data_ptr(), vel.data_ptr(), prs.data_ptr()
+        ws = torch.empty(plan.state_bytes(), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_update_padded(plan.handle, stream, f.data_ptr(),
+                                                f_out.data_ptr(), C.byref(args), C.byref(m),
+                                                ws.data_ptr(), ws.numel()))
+        del keep
+        out = {"f": f_out, "density": rho, "velocity": vel, "pressure": prs}
+        if "wall_mask" in state_padded:
+            out["wall_mask"] = state_padded["wall_mask"]
+        return out
 
     def derivatives(self, state: dict, boundary_inputs: dict) -> dict:
         raise NotImplementedError(

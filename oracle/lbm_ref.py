@@ -21,6 +21,8 @@ operation order one step at a time:
 * ``initial_state``                     -- ``lbm.py:719-745``
 * ``update`` (collide everywhere -> roll -> wall-node swap -> faces ->
   moments with F/2, u=0 in walls)      -- ``lbm.py:899-986``
+* ``stream_padded`` / ``update_padded`` (halo-padded variant used under
+  sharding)                            -- ``lbm.py:270-304, 747-897``
 * ``compute_boundary_fluxes``           -- ``lbm.py:995-1017``
 
 Two face conditions have no counterpart in the reference and are written
@@ -166,6 +168,24 @@ def stream(f, lat: Lattice):
                 fq = np.roll(fq, s, axis=d)
         out[..., q] = fq
     return out
+
+
+def stream_padded(f_pad, lat: Lattice, halo: int = 1):
+    """Shift of every population by e_q read across the halo, interior out --
+    lbm.py:270-304 (no wrap: the halo supplies the neighbours)."""
+    ndim = lat.D
+    out = []
+    for q in range(lat.Q):
+        fq = f_pad[..., q]
+        for d in range(ndim):
+            shift = int(lat.e[q, d])
+            n_d = fq.shape[d] - 2 * halo
+            start = halo - shift
+            sl = [slice(None)] * fq.ndim
+            sl[d] = slice(start, start + n_d)
+            fq = fq[tuple(sl)]
+        out.append(fq)
+    return np.stack(out, axis=-1)
 
 
 def guo_forcing(density, velocity, force, tau, lat: Lattice, mode: str = "x64"):
@@ -418,6 +438,75 @@ class OracleLBM:
         if "wall_mask" in state:
             out["wall_mask"] = state["wall_mask"]
         return out
+
+    # lbm.py:747-897
+    def update_padded(self, state_padded, boundary_inputs, dt=1.0):
+        """Halo-aware step: collide the whole padded block, stream across the
+        halo, wall swap and faces on the interior, outputs re-padded with the
+        input's halo entries."""
+        lat, mode, D = self.lat, self.mode, self.lat.D
+        halo = 1
+        f_pad = _cast(state_padded["f"], mode)
+        interior = tuple(slice(halo, -halo) for _ in range(D))
+        if "wall_mask_update" in boundary_inputs:
+            wall_pad = np.asarray(boundary_inputs["wall_mask_update"]).astype(bool)
+        elif "wall_mask" in state_padded:
+            wall_pad = np.asarray(state_padded["wall_mask"]).astype(bool)
+        else:
+            wall_pad = self.wall_mask
+        pshape = f_pad.shape[:-1]
+        force = boundary_inputs.get("body_force", None)
+        if force is None:
+            force = np.zeros(pshape + (D,), dtype=np.float32)
+        else:
+            force = np.asarray(force)
+            if force.ndim == 1 and force.shape == (D,):
+                force = np.broadcast_to(force, pshape + (D,)).astype(np.float32)
+            elif force.shape != pshape + (D,):
+                force = np.pad(force, [(halo, halo)] * D + [(0, 0)])
+        force = _cast(force, mode)
+
+        density, velocity = macroscopic(f_pad, lat, force, mode)
+        f_eq = equilibrium(density, velocity, lat, mode)
+        f_post = f_pad - (f_pad - f_eq) / self.tau
+        f_post = f_post + guo_forcing(density, velocity, force, self.tau, lat, mode)
+        f_str = stream_padded(f_post, lat, halo)
+        wall = wall_pad[interior]
+        f_bc = np.where(wall[..., None], f_str[..., lat.opp], f_str)
+
+        inlet_p = boundary_inputs.get("inlet_pressure", None)
+        inlet_u = boundary_inputs.get("inlet_velocity", None)
+        outlet_p = boundary_inputs.get("outlet_pressure", None)
+        ia, isd = FACE_MAP[self.inlet_face]
+        oa, osd = FACE_MAP[self.outlet_face]
+        if inlet_p is not None:
+            f_bc = zou_he_pressure_face(f_bc, self._rho_from_pressure(inlet_p), lat,
+                                        ia, isd, wall, mode)
+        elif inlet_u is not None:
+            f_bc = velocity_inlet_face(f_bc, inlet_u, lat, ia, isd, wall, mode)
+        if self.outlet_condition == "zero_gradient":
+            f_bc = zero_gradient_face(f_bc, lat, oa, osd, wall)
+        elif outlet_p is not None:
+            f_bc = zou_he_pressure_face(f_bc, self._rho_from_pressure(outlet_p), lat,
+                                        oa, osd, wall, mode)
+
+        density_new, velocity_new = macroscopic(f_bc, lat, force[interior], mode)
+        velocity_new = np.where(wall[..., None], 0.0, velocity_new).astype(velocity_new.dtype)
+        pressure_new = density_new * (np.float32(lat.cs2) if mode == "f32" else lat.cs2)
+
+        def repad(src, new):
+            # functional .at[interior].set: the result keeps the input's dtype
+            out = np.array(src, copy=True)
+            out[interior] = new
+            return out
+
+        result = {"f": repad(f_pad, f_bc),
+                  "density": repad(state_padded["density"], density_new),
+                  "velocity": repad(state_padded["velocity"], velocity_new),
+                  "pressure": repad(state_padded["pressure"], pressure_new)}
+        if "wall_mask" in state_padded:
+            result["wall_mask"] = state_padded["wall_mask"]
+        return result
 
     def run(self, state, boundary_inputs, n_steps):
         for _ in range(n_steps):

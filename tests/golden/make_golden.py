@@ -297,6 +297,84 @@ def run_case(lbm, jnp, case, mode, seed):
     return out
 
 
+PADDED_CASES = [
+    # update_padded (lbm.py:747-897) on a halo-padded state: the halo is a
+    # periodic pad (what a single device gets) plus, for "foreign" halos, a
+    # perturbation standing in for a neighbour shard's different data
+    dict(name="padded_d3q19_walls_uniform_force", lattice="D3Q19", grid=(5, 4, 6),
+         viscosity=0.1, walls="y", faces=("x_min", "x_max"),
+         bi=dict(body_force="uniform"), halo="foreign"),
+    dict(name="padded_d3q19_zou_he_field_force", lattice="D3Q19", grid=(6, 5, 4),
+         viscosity=0.08, walls="random", faces=("x_min", "x_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0,
+                 body_force="field"), halo="foreign"),
+    dict(name="padded_d3q19_periodic_zou_he_z", lattice="D3Q19", grid=(4, 4, 7),
+         viscosity=0.1, walls=None, faces=("z_min", "z_max"),
+         bi=dict(inlet_pressure=1.0 / 3.0 + 1e-3, outlet_pressure=1.0 / 3.0),
+         halo="periodic"),
+    dict(name="padded_d2q9_walls_field_force", lattice="D2Q9", grid=(7, 6),
+         viscosity=0.07, walls="random", faces=("y_min", "y_max"),
+         bi=dict(body_force="field", inlet_pressure=1.0 / 3.0 + 1e-3), halo="foreign"),
+]
+
+
+def run_padded_case(lbm, jnp, case, mode, seed):
+    """One update_padded call of the reference on a padded state."""
+    rng = np.random.default_rng(seed + 2000)
+    grid = case["grid"]
+    D = len(grid)
+    walls = _walls(case["walls"], grid, rng)
+    node = lbm.LBMNode(name=case["name"], timestep=1.0, grid_shape=grid,
+                       viscosity=case["viscosity"], lattice=case["lattice"],
+                       wall_mask=walls, inlet_face=case["faces"][0],
+                       outlet_face=case["faces"][1])
+    f0 = _perturbed_f(lbm, node, seed)
+    st = node.initial_state()
+    pad = [(1, 1)] * D
+
+    def pad_field(a, extra=0):
+        return np.pad(np.asarray(_plain(a)), pad + [(0, 0)] * extra, mode="wrap")
+
+    f_pad = pad_field(f0, 1)
+    wall_pad = pad_field(np.asarray(_plain(st["wall_mask"])))
+    if case["halo"] == "foreign":
+        inner = tuple(slice(1, -1) for _ in range(D))
+        halo_mask = np.ones(f_pad.shape[:D], dtype=bool)
+        halo_mask[inner] = False
+        w = node._lat.w
+        noise = (1e-3 * w * rng.standard_normal(f_pad.shape)).astype(np.float32)
+        f_pad = np.where(halo_mask[..., None], f_pad + noise, f_pad).astype(np.float32)
+        wall_pad = np.where(halo_mask, rng.random(halo_mask.shape) < 0.3, wall_pad)
+    wall_pad = wall_pad.astype(np.uint8)
+    dens_pad = pad_field(st["density"])
+    vel_pad = pad_field(st["velocity"], 1)
+    prs_pad = pad_field(st["pressure"])
+    f_in = f_pad.astype(np.float64) if mode == "x64" else f_pad
+    state_p = {"f": jnp.asarray(f_in), "density": jnp.asarray(dens_pad),
+               "velocity": jnp.asarray(vel_pad), "pressure": jnp.asarray(prs_pad),
+               "wall_mask": jnp.asarray(wall_pad)}
+    bi, bi_np = {}, {}
+    for k, v in case["bi"].items():
+        if k == "body_force":
+            if v == "uniform":
+                arr = np.array([1e-4, -3e-5, 2e-5][:D], dtype=np.float32)
+            else:   # interior-shaped field: the reference zero-pads it
+                arr = (1e-4 * rng.standard_normal(grid + (D,))).astype(np.float32)
+            bi[k] = jnp.asarray(arr)
+            bi_np[k] = arr
+        else:
+            bi[k] = np.float32(v)
+            bi_np[k] = np.float32(v)
+    out = {"f_pad": f_pad, "wall_pad": wall_pad, "density_pad": dens_pad,
+           "velocity_pad": vel_pad, "pressure_pad": prs_pad, "tau": np.float64(node.tau)}
+    for k, v in bi_np.items():
+        out["bi_" + k] = np.asarray(v)
+    res = node.update_padded(state_p, bi, 1.0)
+    for key in ("f", "density", "velocity", "pressure"):
+        out["out_" + key] = np.asarray(_plain(res[key]))
+    return out
+
+
 def unit_vectors(lbm, jnp, seed=7):
     """Golden vectors for the pure kernels on random inputs (x64)."""
     rng = np.random.default_rng(seed)
@@ -320,6 +398,10 @@ def unit_vectors(lbm, jnp, seed=7):
         out[f"{tag}_macro_rho"] = np.asarray(_plain(d))
         out[f"{tag}_macro_u"] = np.asarray(_plain(v))
         out[f"{tag}_stream"] = np.asarray(_plain(lbm._stream(jnp.asarray(f), lat.e, lat.D)))
+        fpad = np.random.default_rng(seed + lat.Q).random(tuple(n + 2 for n in grid) + (lat.Q,))
+        out[f"{tag}_fpad"] = fpad
+        out[f"{tag}_stream_padded"] = np.asarray(_plain(lbm._stream_padded(
+            jnp.asarray(fpad), lat.e, lat.D, 1)))
         out[f"{tag}_guo"] = np.asarray(_plain(lbm._guo_forcing(
             jnp.asarray(rho), jnp.asarray(u), jnp.asarray(F), 0.73, lat.e, lat.w, lat.cs2)))
         out[f"{tag}_opp_map"] = lbm._get_opp_map(lat.e)
@@ -344,10 +426,16 @@ def main(ref_root="/root/reference"):
             res = run_case(lbm, jnp, case, mode, seed=i)
             for k, v in res.items():
                 golden[f"{case['name']}|{mode}|{k}"] = v
+    for i, case in enumerate(PADDED_CASES):
+        for mode in ("x64", "f32"):
+            MODE["value"] = mode
+            res = run_padded_case(lbm, jnp, case, mode, seed=100 + i)
+            for k, v in res.items():
+                golden[f"{case['name']}|{mode}|{k}"] = v
     MODE["value"] = "x64"
     out = Path(__file__).with_name("lbm_golden.npz")
     np.savez_compressed(out, **golden)
-    meta = {c["name"]: c for c in CASES}
+    meta = {c["name"]: c for c in CASES + PADDED_CASES}
     print(f"wrote {out} ({out.stat().st_size / 1024:.1f} KiB, {len(golden)} arrays, "
           f"{len(meta)} cases)")
 

@@ -105,3 +105,20 @@ def test_update_rejects_missing_workspace_before_any_device_work():
     assert "n_steps" in _lib.last_error()
     rc = lib.lbm_update(p.handle, None, None, fake, C.byref(args), None, fake, 1 << 30)
     assert rc == -1
+
+
+def test_update_padded_rejects_blocks_without_a_halo_before_any_device_work():
+    lib = _lib.lib()
+    args = _lib.lbm_step_args()
+    fake = C.c_void_p(0x1000)  # never dereferenced: validation fails first
+    thin = _lib.Plan(19, (8, 2, 8), 0.8)
+    rc = lib.lbm_update_padded(thin.handle, None, fake, fake, C.byref(args), None, fake, 1 << 30)
+    assert rc == -1 and "halo" in _lib.last_error()
+    p = _lib.Plan(19, (8, 8, 8), 0.8)
+    rc = lib.lbm_update_padded(p.handle, None, fake, fake, C.byref(args), None, fake, 16)
+    assert rc == -4 and "workspace" in _lib.last_error()
+    args.outlet.kind, args.outlet.face = _lib.BC_ZERO_GRADIENT, _lib.FACES["x_max"]
+    short = _lib.Plan(19, (4, 8, 8), 0.8)
+    rc = lib.lbm_update_padded(short.handle, None, fake, fake, C.byref(args), None, fake,
+                               1 << 30)
+    assert rc == -1 and "interior" in _lib.last_error()

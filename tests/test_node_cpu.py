@@ -71,10 +71,13 @@ def test_derivatives_raises():
         node.derivatives({}, {})
 
 
-def test_update_padded_not_provided():
+def test_update_padded_needs_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("has a GPU")
     node = LBMNode(name="lbm", timestep=0.001, grid_shape=(8, 8, 8))
-    with pytest.raises(NotImplementedError):
-        node.update_padded({}, {}, 1.0)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        node.update_padded({"f": np.zeros((10, 10, 10, 19), np.float32)}, {}, 1.0)
 
 
 def test_lattice_descriptors_match_reference_order():
