@@ -690,6 +690,12 @@ struct BatchTile {
 // [1] p in A -> out B, [2] the last step (reference f and moments out).
 constexpr int kBatchArgs = 3;
 
+// Per-instance arguments of a batched tile: staged in shared memory (1), or
+// read from global memory through the L1 (0).
+#ifndef LBM_BATCH_ARGS_SMEM
+#define LBM_BATCH_ARGS_SMEM 0
+#endif
+
 // Copies instance arguments into shared memory (the whole block reads them).
 __device__ __forceinline__ void stage_args(StepArgs& dst, const StepArgs& src) {
   static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied as 32-bit words");
@@ -722,16 +728,22 @@ template <int Q, class S, int MODE, int SPEC>
 __global__ void __launch_bounds__(kBlock, min_blocks<S>())
     k_batched_step(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                    uint32_t ntiles, int which) {
+#if LBM_BATCH_ARGS_SMEM
   __shared__ StepArgs sa;
   uint32_t cur = 0xffffffffu;
+#endif
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BatchTile tile = tiles[t];
+#if LBM_BATCH_ARGS_SMEM
     if (tile.inst != cur) {
       __syncthreads();
       stage_args(sa, args[kBatchArgs * tile.inst + which]);
       __syncthreads();
       cur = tile.inst;
     }
+#else
+    const StepArgs& sa = args[kBatchArgs * tile.inst + which];
+#endif
 #pragma unroll 1
     for (int j = 0; j < kBatchTile / kBlock; ++j) {
       const uint32_t c = tile.first + j * kBlock + threadIdx.x;

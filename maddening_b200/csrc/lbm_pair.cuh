@@ -15,19 +15,18 @@
 // l of a warp owns the aligned pair (k, k+1), k = first + 2 l.  The pull
 // along the contiguous axis:
 //   c2 =  0: both cells read the thread's own pair;
-//   c2 = +1: cell k reads k - 1, the high half of lane l-1's pair (shuffle
-//            up); lane 0 loads the pair before the warp's segment itself
-//            (periodic wrap at the row start); cell k+1 reads the low half of
-//            its own pair;
-//   c2 = -1: mirror image (shuffle down; lane 31 loads the pair after).
+//   c2 = +1: cell k reads k - 1, the high half of the pair before (a second
+//            aligned word, wrapped at the row start; the neighbouring lane
+//            loads the same line, so it hits L1); cell k+1 reads the low half
+//            of its own pair;
+//   c2 = -1: mirror image (the pair after, wrapped at the row end).
 // After the pull each cell runs exactly the arithmetic of the one-cell step
 // (wall swap -> faces -> moments -> collide), so the results are
 // bit-identical; the wall swap is skipped by warps without a wall cell and the
 // face checks by pairs that cannot touch a face.
 //
 // A second form (k_step_gpair) takes any even row length: pairs follow the
-// instance-wide cell index, each lane finds its own row, and the lanes whose
-// neighbour pair lies in another row or outside the warp load it themselves.
+// instance-wide cell index and each lane finds its own row.
 //
 // Requirements (checked on the host): an even contiguous extent n2 (a multiple
 // of 64 W for the row-segment form), state planes and the wall mask aligned for
@@ -54,8 +53,6 @@ struct PairT<__half> {
   static __device__ __forceinline__ float hi(P v) {
     return __high2float(*reinterpret_cast<const __half2*>(&v));
   }
-  static __device__ __forceinline__ P shup(P v) { return __shfl_up_sync(0xffffffffu, v, 1); }
-  static __device__ __forceinline__ P shdn(P v) { return __shfl_down_sync(0xffffffffu, v, 1); }
   static __device__ __forceinline__ void st(__half* p, float a, float b) {
     const __half2 h = __floats2half2_rn(a, b);
     *reinterpret_cast<unsigned int*>(p) = *reinterpret_cast<const unsigned int*>(&h);
@@ -70,8 +67,6 @@ struct PairT<__nv_bfloat16> {
   }
   static __device__ __forceinline__ float lo(P v) { return __uint_as_float(v << 16); }
   static __device__ __forceinline__ float hi(P v) { return __uint_as_float(v & 0xffff0000u); }
-  static __device__ __forceinline__ P shup(P v) { return __shfl_up_sync(0xffffffffu, v, 1); }
-  static __device__ __forceinline__ P shdn(P v) { return __shfl_down_sync(0xffffffffu, v, 1); }
   static __device__ __forceinline__ void st(__nv_bfloat16* p, float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     *reinterpret_cast<unsigned int*>(p) = *reinterpret_cast<const unsigned int*>(&h);
@@ -86,13 +81,6 @@ struct PairT<float> {
   }
   static __device__ __forceinline__ float lo(P v) { return v.x; }
   static __device__ __forceinline__ float hi(P v) { return v.y; }
-  static __device__ __forceinline__ P shup(P v) {
-    return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
-  }
-  static __device__ __forceinline__ P shdn(P v) {
-    return make_float2(__shfl_down_sync(0xffffffffu, v.x, 1),
-                       __shfl_down_sync(0xffffffffu, v.y, 1));
-  }
   static __device__ __forceinline__ void st(float* p, float a, float b) {
     *reinterpret_cast<float2*>(p) = make_float2(a, b);
   }
@@ -118,18 +106,17 @@ __device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, floa
 }
 
 // Everything after the plane loads of one thread's pair (k, k+1) of row
-// `rbase`: lane l's own pair words v[q]; e[q] the word of the pair before
-// (c2 > 0, lanes with edge_prev) or after (c2 < 0, lanes with edge_next) for
-// the lanes whose neighbour pair is not held by the adjacent lane.  All 32
-// lanes of the warp must call it (shuffles, vote); `store` = false for lanes
-// that only pad the warp.
+// `rbase`: v[q] the pair word at (k, k+1) of the source row of direction q,
+// e[q] the word of the pair before (c2 > 0: cell k pulls k - 1) or after
+// (c2 < 0: cell k + 1 pulls k + 2), periodic along the row.  All 32 lanes of
+// the warp must call it (vote); `store` = false for lanes that only pad the
+// warp.
 template <int Q, class S, bool FACES, bool FORCE>
 __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint32_t i1,
-                                            uint32_t k, uint32_t rbase, bool edge_prev,
-                                            bool edge_next, const typename PairT<S>::P (&v)[Q],
+                                            uint32_t k, uint32_t rbase,
+                                            const typename PairT<S>::P (&v)[Q],
                                             const typename PairT<S>::P (&e)[Q], bool store) {
   using PT = PairT<S>;
-  using P = typename PT::P;
   const Geo& g = a.g;
   float da[Q], db[Q];
 #pragma unroll
@@ -139,15 +126,11 @@ __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint
       da[q] = PT::lo(v[q]);
       db[q] = PT::hi(v[q]);
     } else if (c2 > 0) {
-      P nb = PT::shup(v[q]);
-      if (edge_prev) nb = e[q];
-      da[q] = PT::hi(nb);
+      da[q] = PT::hi(e[q]);
       db[q] = PT::lo(v[q]);
     } else {
-      P nb = PT::shdn(v[q]);
-      if (edge_next) nb = e[q];
       da[q] = PT::hi(v[q]);
-      db[q] = PT::lo(nb);
+      db[q] = PT::lo(e[q]);
     }
   }
   bool wa = false, wb = false;
@@ -207,12 +190,10 @@ __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
   const uint32_t row = blockIdx.x;
   const uint32_t i0 = fdiv(row, g.div_n1);
   const uint32_t i1 = row - i0 * g.n1;
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t wfirst = blockIdx.y * (64u * W) + (threadIdx.x >> 5) * 64u;
-  const uint32_t k = wfirst + 2u * lane;
-  // pair before / after this warp's segment (periodic along the row)
-  const uint32_t kprev = (wfirst == 0 ? g.n2 : wfirst) - 2u;
-  const uint32_t knext = wfirst + 64u == g.n2 ? 0u : wfirst + 64u;
+  const uint32_t k = blockIdx.y * (64u * W) + 2u * threadIdx.x;
+  // pair before / after this thread's pair (periodic along the row)
+  const uint32_t kprev = (k == 0 ? g.n2 : k) - 2u;
+  const uint32_t knext = k + 2u == g.n2 ? 0u : k + 2u;
   // source rows of the pull x - e_q (periodic)
   const uint32_t i0m = i0 == 0 ? g.n0 - 1 : i0 - 1, i0p = i0 + 1 == g.n0 ? 0u : i0 + 1;
   const uint32_t i1m = i1 == 0 ? g.n1 - 1 : i1 - 1, i1p = i1 + 1 == g.n1 ? 0u : i1 + 1;
@@ -227,16 +208,15 @@ __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
     const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
     const S* base = pin + (static_cast<uint32_t>(q) * g.ncell + (s0 * g.n1 + s1) * g.n2);
     v[q] = PT::ld(base + k);
-    if (c2 > 0 && lane == 0) e[q] = PT::ld(base + kprev);
-    if (c2 < 0 && lane == 31) e[q] = PT::ld(base + knext);
+    if (c2 > 0) e[q] = PT::ld(base + kprev);
+    if (c2 < 0) e[q] = PT::ld(base + knext);
   }
-  pair_finish<Q, S, FACES, FORCE>(a, i0, i1, k, row * g.n2, lane == 0, lane == 31, v, e, true);
+  pair_finish<Q, S, FACES, FORCE>(a, i0, i1, k, row * g.n2, v, e, true);
 }
 
 // Pairs of one instance-wide index: pair j holds cells 2j, 2j + 1 (rows of even
 // length, so a pair never spans two rows).  Row coordinates and source rows
-// are per lane; a lane whose neighbour pair lies in another row (k = 0 or
-// k + 2 = n2) or outside the warp loads it itself.
+// are per lane.
 template <int Q, class S, bool FACES, bool FORCE>
 __device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
   using PT = PairT<S>;
@@ -245,13 +225,10 @@ __device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
   const uint32_t npairs = g.ncell >> 1;
   const bool valid = pidx < npairs;
   const Cell x = locate(g, 2u * (valid ? pidx : npairs - 1u));
-  const uint32_t lane = threadIdx.x & 31u;
   const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
   const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
   const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.n2 : 0u - g.n2;  // i1 - 1
   const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.n2 : g.n2;
-  const bool edge_prev = lane == 0 || x.k == 0;
-  const bool edge_next = lane == 31 || x.k + 2 == g.n2;
   const uint32_t kprev = (x.k == 0 ? g.n2 : x.k) - 2u;
   const uint32_t knext = x.k + 2 == g.n2 ? 0u : x.k + 2;
   const S* pin = static_cast<const S*>(a.pin);
@@ -267,10 +244,10 @@ __device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
     if (c1 < 0) off += dp1;
     const S* base = pin + (static_cast<uint32_t>(q) * g.ncell + off);
     v[q] = PT::ld(base + x.k);
-    if (c2 > 0 && edge_prev) e[q] = PT::ld(base + kprev);
-    if (c2 < 0 && edge_next) e[q] = PT::ld(base + knext);
+    if (c2 > 0) e[q] = PT::ld(base + kprev);
+    if (c2 < 0) e[q] = PT::ld(base + knext);
   }
-  pair_finish<Q, S, FACES, FORCE>(a, x.i0, x.i1, x.k, x.row, edge_prev, edge_next, v, e, valid);
+  pair_finish<Q, S, FACES, FORCE>(a, x.i0, x.i1, x.k, x.row, v, e, valid);
 }
 
 template <int Q, class S, bool FACES, bool FORCE>
@@ -286,16 +263,22 @@ template <int Q, class S, int SPEC>
 __global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
     k_batched_pair(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                    uint32_t ntiles, int which) {
+#if LBM_BATCH_ARGS_SMEM
   __shared__ StepArgs sa;
   uint32_t cur = 0xffffffffu;
+#endif
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const BatchTile tile = tiles[t];
+#if LBM_BATCH_ARGS_SMEM
     if (tile.inst != cur) {
       __syncthreads();
       stage_args(sa, args[kBatchArgs * tile.inst + which]);
       __syncthreads();
       cur = tile.inst;
     }
+#else
+    const StepArgs& sa = args[kBatchArgs * tile.inst + which];
+#endif
 #pragma unroll 1
     for (int j = 0; j < kBatchTile / (2 * kBlock); ++j) {
       const uint32_t pidx = (tile.first >> 1) + j * kBlock + threadIdx.x;
