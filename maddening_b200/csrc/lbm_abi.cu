@@ -601,20 +601,23 @@ int adj_backward(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void*
 // together; grid = blocks of the persistent launch for that range; pair = its
 // state steps run the paired kernel (16-bit storage, even rows).
 struct TileRange {
-  uint32_t t0, t1;
-  unsigned grid;
-  bool pair;
+  uint32_t t0, t1;  // reference-layout tiles (prepare, one-cell steps, last step)
+  uint32_t s0, s1;  // state-layout tiles (paired state steps)
+  unsigned grid, sgrid;
+  bool pair;        // state steps paired
+  bool pad;         // ... with padded state rows
 };
 
 // Prepare pass over all tiles, then for each instance group its n - 1 state
 // steps and its last step.  A group whose two population copies fit in L2
 // stays there for all of its steps.
 template <int Q, class S, int MODE, int SPEC>
-void batched_launch(bool pair, const lbm::StepArgs* args, const lbm::BatchTile* t, uint32_t nt,
-                    unsigned grid, int which, cudaStream_t s) {
+void batched_launch(bool pair, bool pad, const lbm::StepArgs* args, const lbm::BatchTile* t,
+                    uint32_t nt, unsigned grid, int which, cudaStream_t s) {
   if constexpr (MODE == lbm::kOutState && sizeof(S) == 2) {
     if (pair) {
-      lbm::k_batched_pair<Q, S, SPEC><<<grid, lbm::kBlock, 0, s>>>(args, t, nt, which);
+      if (pad) lbm::k_batched_pair<Q, S, SPEC, true><<<grid, lbm::kBlock, 0, s>>>(args, t, nt, which);
+      else lbm::k_batched_pair<Q, S, SPEC, false><<<grid, lbm::kBlock, 0, s>>>(args, t, nt, which);
       return;
     }
   }
@@ -623,21 +626,22 @@ void batched_launch(bool pair, const lbm::StepArgs* args, const lbm::BatchTile* 
 
 // spec: 0 = per-tile run-time choice, else 1 + 2 FACES + FORCE shared by all members
 template <int Q, class S, int MODE>
-void batched_step(int spec, bool pair, const lbm::StepArgs* args, const lbm::BatchTile* t,
-                  uint32_t nt, unsigned grid, int which, cudaStream_t s) {
+void batched_step(int spec, bool pair, bool pad, const lbm::StepArgs* args,
+                  const lbm::BatchTile* t, uint32_t nt, unsigned grid, int which, cudaStream_t s) {
   switch (spec) {
-    case 1: batched_launch<Q, S, MODE, 1>(pair, args, t, nt, grid, which, s); break;
-    case 2: batched_launch<Q, S, MODE, 2>(pair, args, t, nt, grid, which, s); break;
-    case 3: batched_launch<Q, S, MODE, 3>(pair, args, t, nt, grid, which, s); break;
-    case 4: batched_launch<Q, S, MODE, 4>(pair, args, t, nt, grid, which, s); break;
-    default: batched_launch<Q, S, MODE, 0>(pair, args, t, nt, grid, which, s); break;
+    case 1: batched_launch<Q, S, MODE, 1>(pair, pad, args, t, nt, grid, which, s); break;
+    case 2: batched_launch<Q, S, MODE, 2>(pair, pad, args, t, nt, grid, which, s); break;
+    case 3: batched_launch<Q, S, MODE, 3>(pair, pad, args, t, nt, grid, which, s); break;
+    case 4: batched_launch<Q, S, MODE, 4>(pair, pad, args, t, nt, grid, which, s); break;
+    default: batched_launch<Q, S, MODE, 0>(pair, pad, args, t, nt, grid, which, s); break;
   }
 }
 
 template <int Q, class S>
-int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t ntiles,
-                unsigned grid_all, const std::vector<TileRange>& groups, int64_t n,
-                cudaStream_t s, cudaStream_t side, bool use_graph, int spec) {
+int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles,
+                const lbm::BatchTile* stiles, uint32_t ntiles, unsigned grid_all,
+                const std::vector<TileRange>& groups, int64_t n, cudaStream_t s,
+                cudaStream_t side, bool use_graph, int spec) {
   lbm::k_batched_prepare<Q, S><<<grid_all, lbm::kBlock, 0, s>>>(args, tiles, ntiles);
   int rc = cuda_check(cudaGetLastError(), "k_batched_prepare launch");
   if (rc) return rc;
@@ -655,10 +659,15 @@ int batched_run(const lbm::StepArgs* args, const lbm::BatchTile* tiles, uint32_t
   for (const TileRange& r : groups) {
     const lbm::BatchTile* t = tiles + r.t0;
     const uint32_t nt = r.t1 - r.t0;
-    for (int64_t k = 1; k < n; ++k)
-      batched_step<Q, S, lbm::kOutState>(spec, r.pair, args, t, nt, r.grid,
-                                         static_cast<int>(k % 2), ls);
-    batched_step<Q, S, lbm::kOutAoS>(spec, false, args, t, nt, r.grid, 2, ls);
+    for (int64_t k = 1; k < n; ++k) {
+      if (r.pair)
+        batched_step<Q, S, lbm::kOutState>(spec, true, r.pad, args, stiles + r.s0, r.s1 - r.s0,
+                                           r.sgrid, static_cast<int>(k % 2), ls);
+      else
+        batched_step<Q, S, lbm::kOutState>(spec, false, false, args, t, nt, r.grid,
+                                           static_cast<int>(k % 2), ls);
+    }
+    batched_step<Q, S, lbm::kOutAoS>(spec, false, false, args, t, nt, r.grid, 2, ls);
   }
   rc = cuda_check(cudaGetLastError(), "k_batched_step launch");
   if (use_graph) {
@@ -682,16 +691,21 @@ constexpr int kTileOrders = 3;
 struct lbm_batch {
   int n = 0, Q = 0, D = 0, storage = 0;
   std::vector<const lbm_plan*> plans;
+  std::vector<lbm::Geo> sgeo;     // member geometry with its state-plane layout
   std::vector<size_t> state_off;  // instance i: two population copies at this offset
-  size_t args_off = 0, tiles_off[kTileOrders] = {0, 0, 0}, total = 0;
+  size_t args_off = 0, tiles_off[kTileOrders] = {0, 0, 0}, stiles_off[kTileOrders] = {0, 0, 0};
+  size_t total = 0;
   // [0] instance-major in member order, [1] round-robin across members,
-  // [2] instance-major from the smallest member to the largest
-  std::vector<lbm::BatchTile> tiles[kTileOrders];
-  // members in the order of tile lists 0 and 2 (members whose state steps can
-  // run paired -- 16-bit storage, even rows -- first), with their first tile
+  // [2] instance-major from the smallest member to the largest; tiles over the
+  // reference layout (tiles) and over the state planes (stiles; they differ
+  // for padded rows)
+  std::vector<lbm::BatchTile> tiles[kTileOrders], stiles[kTileOrders];
+  // members in the order of tile lists 0 and 2 (members whose state steps run
+  // paired -- 16-bit storage -- first), with their first tile in each list
   std::vector<int> order[kTileOrders];
-  std::vector<uint32_t> first_tile[kTileOrders];
-  int npair = 0;  // number of those members
+  std::vector<uint32_t> first_tile[kTileOrders], first_stile[kTileOrders];
+  int npair = 0;  // number of those members: the first npair_even have even rows
+  int npair_even = 0;
   cudaStream_t side = nullptr;
 };
 
@@ -787,6 +801,10 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
   p->g.ncell = static_cast<uint32_t>(ncell);
   p->g.div_n2 = make_fastdiv(p->g.n2);
   p->g.div_n1 = make_fastdiv(p->g.n1);
+  p->g.rstride = p->g.n2;
+  p->g.splane = p->g.plane;
+  p->g.pstride = p->g.ncell;
+  p->g.div_rstride = p->g.div_n2;
   if (!fastdiv_ok(p->g.div_n2, p->g.ncell) ||
       !fastdiv_ok(p->g.div_n1, static_cast<uint32_t>(dims[0] * dims[1]))) {
     delete p;
@@ -985,8 +1003,10 @@ int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
   size_t o = 0;
   b->args_off = o;
   o += align256(sizeof(lbm::StepArgs) * lbm::kBatchArgs * static_cast<size_t>(n));
-  std::vector<std::vector<lbm::BatchTile>> per(n);
-  size_t ntiles = 0;
+  const bool half = b->storage == LBM_STORE_F16 || b->storage == LBM_STORE_BF16;
+  auto pairable = [&](int i) { return half && !(plans[i]->flags & LBM_PLAN_SINGLE_CELLS); };
+  std::vector<std::vector<lbm::BatchTile>> per(n), sper(n);
+  size_t ntiles = 0, nstiles = 0;
   for (int i = 0; i < n; ++i) {
     const lbm_plan* p = plans[i];
     if (p == nullptr || p->Q != b->Q || p->storage != b->storage) {
@@ -994,34 +1014,55 @@ int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
       return fail(LBM_ERR_INVALID, "instance %d: plans must share lattice and storage", i);
     }
     b->plans.push_back(p);
-    for (uint32_t c = 0; c < p->g.ncell; c += lbm::kBatchTile)
+    // A paired member with odd rows keeps its state rows padded to n2 + 1.
+    lbm::Geo g = p->g;
+    if (pairable(i) && g.n2 % 2 == 1) {
+      const uint64_t rs = uint64_t(g.n2) + 1;
+      const uint64_t ps = uint64_t(g.n0) * g.n1 * rs;
+      g.rstride = static_cast<uint32_t>(rs);
+      g.splane = static_cast<uint32_t>(uint64_t(g.n1) * rs);
+      g.div_rstride = make_fastdiv(g.rstride);
+      if (ps * p->Q >= (uint64_t(1) << 32) || !fastdiv_ok(g.div_rstride, static_cast<uint32_t>(ps))) {
+        delete b;
+        return fail(LBM_ERR_INVALID, "instance %d: padded rows exceed 32-bit indexing", i);
+      }
+      g.pstride = static_cast<uint32_t>(ps);
+    }
+    b->sgeo.push_back(g);
+    for (uint32_t c = 0; c < g.ncell; c += lbm::kBatchTile)
       per[i].push_back(lbm::BatchTile{static_cast<uint32_t>(i), c});
+    for (uint32_t c = 0; c < g.pstride; c += lbm::kBatchTile)
+      sper[i].push_back(lbm::BatchTile{static_cast<uint32_t>(i), c});
     ntiles += per[i].size();
+    nstiles += sper[i].size();
   }
-  if (ntiles >= (size_t(1) << 31)) {
+  if (nstiles >= (size_t(1) << 31)) {
     delete b;
     return fail(LBM_ERR_INVALID, "ensemble too large");
   }
-  auto pairable = [&](int i) {
-    return (b->storage == LBM_STORE_F16 || b->storage == LBM_STORE_BF16) &&
-           plans[i]->g.n2 % 2 == 0 && !(plans[i]->flags & LBM_PLAN_SINGLE_CELLS);
-  };
   std::vector<int> by_member(n), by_size(n);
   for (int i = 0; i < n; ++i) by_member[i] = by_size[i] = i;
   std::stable_sort(by_size.begin(), by_size.end(),
                    [&](int x, int y) { return plans[x]->g.ncell < plans[y]->g.ncell; });
+  // classes: paired with even rows, paired with padded rows, one cell
+  auto cls = [&](int i) { return !pairable(i) ? 2 : (plans[i]->g.n2 % 2 == 0 ? 0 : 1); };
   for (auto* v : {&by_member, &by_size})
-    std::stable_partition(v->begin(), v->end(), pairable);
-  for (int i = 0; i < n; ++i) b->npair += pairable(i) ? 1 : 0;
+    std::stable_sort(v->begin(), v->end(), [&](int x, int y) { return cls(x) < cls(y); });
+  for (int i = 0; i < n; ++i) {
+    b->npair += cls(i) < 2 ? 1 : 0;
+    b->npair_even += cls(i) == 0 ? 1 : 0;
+  }
   for (int k : {0, 2}) {
     for (int j = 0; j < n; ++j) {
       const int i = k == 0 ? by_member[j] : by_size[j];
       b->order[k].push_back(i);
       b->first_tile[k].push_back(static_cast<uint32_t>(b->tiles[k].size()));
+      b->first_stile[k].push_back(static_cast<uint32_t>(b->stiles[k].size()));
       b->tiles[k].insert(b->tiles[k].end(), per[i].begin(), per[i].end());
+      b->stiles[k].insert(b->stiles[k].end(), sper[i].begin(), sper[i].end());
     }
   }
-  for (size_t r = 0;; ++r) {  // round-robin across instances
+  for (size_t r = 0;; ++r) {  // round-robin across instances (one-cell steps only)
     bool any = false;
     for (int i = 0; i < n; ++i)
       if (r < per[i].size()) { b->tiles[1].push_back(per[i][r]); any = true; }
@@ -1030,10 +1071,13 @@ int lbm_batch_create(const lbm_plan* const* plans, int32_t n, lbm_batch** out) {
   for (int k = 0; k < kTileOrders; ++k) {
     b->tiles_off[k] = o;
     o += align256(sizeof(lbm::BatchTile) * ntiles);
+    b->stiles_off[k] = o;
+    o += align256(sizeof(lbm::BatchTile) * (k == 1 ? 1 : nstiles));
   }
   for (int i = 0; i < n; ++i) {
     b->state_off.push_back(o);
-    o += 2 * align256(state_bytes(plans[i]));
+    const size_t sb = static_cast<size_t>(b->Q) * b->sgeo[i].pstride * plans[i]->elem;
+    o += 2 * align256(sb);
   }
   b->total = o;
   if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess) b->side = nullptr;
@@ -1080,8 +1124,9 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
     lbm::StepArgs a;
     int rc = build_args(p, &args[i], out != nullptr ? &out[i] : nullptr, &a);
     if (rc) return rc;
+    a.g = b->sgeo[i];  // the member's state-plane layout (padded rows or not)
     char* A = ws + b->state_off[i];
-    char* B = A + align256(state_bytes(p));
+    char* B = A + align256(static_cast<size_t>(b->Q) * a.g.pstride * p->elem);
     lbm::StepArgs m = a;
     m.rho = m.vel = m.prs = nullptr;
     m.f_in = f_in[i];
@@ -1107,13 +1152,20 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   lbm::StepArgs* dargs = reinterpret_cast<lbm::StepArgs*>(ws + b->args_off);
   lbm::BatchTile* dtiles = reinterpret_cast<lbm::BatchTile*>(ws + b->tiles_off[c.tile_order]);
+  lbm::BatchTile* dstiles = reinterpret_cast<lbm::BatchTile*>(ws + b->stiles_off[c.tile_order]);
   const auto& tl = b->tiles[c.tile_order];
+  const auto& stl = b->stiles[c.tile_order];
   int rc = cuda_check(cudaMemcpyAsync(dargs, host.data(), host.size() * sizeof(lbm::StepArgs),
                                       cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
   if (rc) return rc;
   rc = cuda_check(cudaMemcpyAsync(dtiles, tl.data(), tl.size() * sizeof(lbm::BatchTile),
                                   cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
   if (rc) return rc;
+  if (!stl.empty()) {
+    rc = cuda_check(cudaMemcpyAsync(dstiles, stl.data(), stl.size() * sizeof(lbm::BatchTile),
+                                    cudaMemcpyHostToDevice, s), "cudaMemcpyAsync");
+    if (rc) return rc;
+  }
   const uint32_t ntiles = static_cast<uint32_t>(tl.size());
   unsigned cap = 0;  // persistent grid size, 0 = one block per tile
   if (c.blocks_per_sm > 0) {
@@ -1127,42 +1179,59 @@ int lbm_batch_rollout(const lbm_batch* b, lbm_stream_t stream, const void* const
   // population copies together stay within group_mib (a member larger than
   // that is a group of its own); 0 = all members in every launch.
   // Members whose state steps run paired come first in tile orders 0 and 2;
-  // their wall masks must be 2-byte aligned (else nothing runs paired).
+  // members with even rows read their wall mask two bytes at a time, so it
+  // must be 2-byte aligned (else nothing runs paired).
   int npair = c.tile_order == 1 ? 0 : b->npair;
   for (int j = 0; j < npair; ++j) {
     const int i = b->order[c.tile_order][j];
-    if (reinterpret_cast<uintptr_t>(args[i].wall) % 2 != 0) npair = 0;
+    if (b->sgeo[i].rstride == b->sgeo[i].n2 && reinterpret_cast<uintptr_t>(args[i].wall) % 2 != 0)
+      npair = 0;
   }
+  const size_t jeven = npair > 0 ? static_cast<size_t>(b->npair_even) : 0u;
   std::vector<TileRange> groups;
   const auto& ord = b->order[c.tile_order];
   const auto& ft = b->first_tile[c.tile_order];
-  const uint32_t tsplit = npair > 0 && npair < b->n ? ft[npair] : (npair > 0 ? ntiles : 0u);
-  auto add_range = [&](uint32_t t0, uint32_t t1, bool pair) {
-    if (t1 > t0) groups.push_back(TileRange{t0, t1, grid_for_tiles(t1 - t0), pair});
+  const auto& fs = b->first_stile[c.tile_order];
+  const uint32_t nstiles = static_cast<uint32_t>(stl.size());
+  // member j of the order -> its first reference / state tile (end = totals)
+  auto tile_at = [&](size_t j) { return j < ord.size() ? ft[j] : ntiles; };
+  auto stile_at = [&](size_t j) { return j < ord.size() ? fs[j] : nstiles; };
+  const size_t jsplit = static_cast<size_t>(npair);
+  // members [0, jeven) paired, [jeven, jsplit) paired with padded rows, the rest one cell
+  auto add_range = [&](size_t j0, size_t j1) {
+    const uint32_t t0 = tile_at(j0), t1 = tile_at(j1);
+    if (t1 <= t0) return;
+    const bool pair = j0 < jsplit, pad = pair && j0 >= jeven;
+    const uint32_t s0 = pair ? stile_at(j0) : 0u, s1 = pair ? stile_at(j1) : 0u;
+    groups.push_back(TileRange{t0, t1, s0, s1, grid_for_tiles(t1 - t0),
+                               grid_for_tiles(s1 - s0), pair, pad});
   };
-  if (c.group_mib == 0) {
-    add_range(0, tsplit, true);
-    add_range(tsplit, ntiles, false);
+  if (c.tile_order == 1) {
+    groups.push_back(TileRange{0, ntiles, 0, 0, grid_for_tiles(ntiles), 0, false, false});
+  } else if (c.group_mib == 0) {
+    add_range(0, jeven);
+    add_range(jeven, jsplit);
+    add_range(jsplit, ord.size());
   } else {
     const size_t budget = static_cast<size_t>(c.group_mib) << 20;
-    size_t used = 0;
-    uint32_t t0 = 0;
+    size_t used = 0, j0 = 0;
     for (size_t j = 0; j < ord.size(); ++j) {
-      const size_t need = 2 * align256(state_bytes(b->plans[ord[j]]));
-      const bool split = static_cast<int>(j) == npair;  // pair / one-cell boundary
-      if (j > 0 && (used + need > budget || split)) {
-        add_range(t0, ft[j], static_cast<int>(j) <= npair);
-        t0 = ft[j];
+      const size_t need =
+          2 * align256(static_cast<size_t>(b->Q) * b->sgeo[ord[j]].pstride * b->plans[ord[j]]->elem);
+      if (j > 0 && (used + need > budget || j == jeven || j == jsplit)) {
+        add_range(j0, j);
+        j0 = j;
         used = 0;
       }
       used += need;
     }
-    add_range(t0, ntiles, static_cast<int>(ord.size()) <= npair);
+    add_range(j0, ord.size());
   }
   const unsigned grid_all = grid_for_tiles(ntiles);
   const bool g = c.use_graph != 0;
 #define LBM_BATCH_RUN(QQ, SS) \
-  batched_run<QQ, SS>(dargs, dtiles, ntiles, grid_all, groups, n_steps, s, b->side, g, spec)
+  batched_run<QQ, SS>(dargs, dtiles, dstiles, ntiles, grid_all, groups, n_steps, s, b->side, \
+                      g, spec)
   switch (b->storage) {
     case LBM_STORE_F32: return b->Q == 19 ? LBM_BATCH_RUN(19, float) : LBM_BATCH_RUN(9, float);
     case LBM_STORE_F16: return b->Q == 19 ? LBM_BATCH_RUN(19, __half) : LBM_BATCH_RUN(9, __half);

@@ -101,6 +101,13 @@ struct Geo {
   uint32_t plane;       // n1 * n2
   uint32_t ncell;       // n0 * n1 * n2
   FastDiv div_n2, div_n1;
+  // Layout of the population planes of the state: row stride, plane stride
+  // (n1 rows) and plane size.  Equal to n2, plane, ncell, except for a
+  // batched member whose rows are padded to an even length (n2 + 1) so that
+  // it can run the paired step; the padding cell of a row is never read.
+  // Reference-layout arrays (f in/out, wall, force, moments) stay unpadded.
+  uint32_t rstride, splane, pstride;
+  FastDiv div_rstride;
 };
 
 struct StepArgs {
@@ -263,7 +270,8 @@ __device__ __forceinline__ Mom<R> moments(const R (&d)[Q], const R (&F)[3]) {
 //         = (1 - omega) d_q + A_q + B_q
 // with the even part A_q = omega (rho' - 1.5 rho u^2 + 4.5 rho eu^2)
 // + c (9 eu eF - 3 u.F) and the odd part B_q = 3 omega rho eu + 3 c eF, so a
-// direction and its opposite share A and negate B.
+// direction and its opposite share A and negate B.  Without a force the
+// velocity terms fold into one product, eu (4.5 omega rho eu +- 3 omega rho).
 template <int Q, class R, bool FORCE>
 __device__ __forceinline__ void collide(R (&d)[Q], const Mom<R>& m, const R (&F)[3], R omega,
                                         R guo_c) {
@@ -289,16 +297,20 @@ __device__ __forceinline__ void collide(R (&d)[Q], const Mom<R>& m, const R (&F)
     const int o = Lat<Q>::opp(q);
     const int e0 = Lat<Q>::c0(q), e1 = Lat<Q>::c1(q), e2 = Lat<Q>::c2(q);
     const R eu = dot_e(e0, e1, e2, m.u);
-    R A = fma_r(r45, mul_r(eu, eu), base);
-    R B = mul_r(r3, eu);
+    const R dq = d[q], dop = d[o];
     if constexpr (FORCE) {
+      R A = fma_r(r45, mul_r(eu, eu), base);
+      R B = mul_r(r3, eu);
       const R eF = dot_e(e0, e1, e2, F);
       A = add_r(A, fma_r(mul_r(c9, eu), eF, -cuF));
       B = fma_r(c3, eF, B);
+      d[q] = add_r(fma_r(keep, dq, A), B);
+      d[o] = sub_r(fma_r(keep, dop, A), B);
+    } else {
+      // (1 - omega) d + base + eu (4.5 omega rho eu +- 3 omega rho)
+      d[q] = fma_r(eu, fma_r(r45, eu, r3), fma_r(keep, dq, base));
+      d[o] = fma_r(eu, fma_r(r45, eu, -r3), fma_r(keep, dop, base));
     }
-    const R dq = d[q], dop = d[o];
-    d[q] = add_r(fma_r(keep, dq, A), B);
-    d[o] = sub_r(fma_r(keep, dop, A), B);
   }
 }
 
@@ -386,7 +398,7 @@ __device__ __forceinline__ typename StoreT<S>::R fbc_at(const StepArgs& a, int q
   const uint32_t j1 = wrapu(i1 + s * Lat<Q>::c1(q), g.n1);
   const uint32_t j2 = wrapu(k + s * Lat<Q>::c2(q), g.n2);
   return ld_pop<S>(static_cast<const S*>(a.pin) +
-                   (static_cast<uint32_t>(qs) * g.ncell + (j0 * g.n1 + j1) * g.n2 + j2));
+                   (static_cast<uint32_t>(qs) * g.pstride + (j0 * g.n1 + j1) * g.rstride + j2));
 }
 
 // Zero-gradient face (extension): unknown q <- f_bc of the neighbour one
@@ -411,26 +423,30 @@ __device__ __forceinline__ void face_zero_gradient(typename StoreT<S>::R (&d)[Q]
 // Kernels
 // ---------------------------------------------------------------------------
 
-// Launch shape of the step kernels: 128 threads, >= 8 blocks per SM (<= 64
-// registers, 32 resident warps); the fastest shape of a B200 sweep.
+// Launch shape of the step kernels: 128 threads, >= 10 blocks per SM (<= 51
+// registers, 40 resident warps); the fastest shape of a B200 sweep.
 #ifndef LBM_STEP_BLOCK
 #define LBM_STEP_BLOCK 128
 #endif
 #ifndef LBM_STEP_MINB
-#define LBM_STEP_MINB 8
+#define LBM_STEP_MINB 10
 #endif
 constexpr int kBlock = LBM_STEP_BLOCK;
 constexpr int kMinBlocks = LBM_STEP_MINB;
 // FP64 arithmetic holds twice the registers: half the resident blocks.
 template <class S>
 constexpr int min_blocks() { return sizeof(typename StoreT<S>::R) == 8 ? kMinBlocks / 2 : kMinBlocks; }
+// The batched kernels also hold a member's arguments: 8 blocks (64 registers).
+template <class S>
+constexpr int batched_min_blocks() { return sizeof(typename StoreT<S>::R) == 8 ? 4 : 8; }
 
 enum StepMode : int { kOutState = 0, kOutAoS = 1, kOutMoments = 2 };
 
 struct Cell {
-  uint32_t c;      // linear cell index
+  uint32_t c;      // linear cell index (reference layout)
   uint32_t i0, i1, k;
   uint32_t row;    // c - k
+  uint32_t srow;   // start of the row in the state planes
 };
 
 __device__ __forceinline__ Cell locate(const Geo& g, uint32_t c) {
@@ -441,6 +457,7 @@ __device__ __forceinline__ Cell locate(const Geo& g, uint32_t c) {
   x.i0 = fdiv(r, g.div_n1);
   x.i1 = r - x.i0 * g.n1;
   x.row = c - x.k;
+  x.srow = r * g.rstride;
   return x;
 }
 
@@ -493,6 +510,9 @@ template <int Q, class S, bool FORCE>
 __device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
+  // index in the state planes (differs only for padded rows)
+  const uint32_t ci =
+      a.g.rstride == a.g.n2 ? c : c + fdiv(c, a.g.div_n2) * (a.g.rstride - a.g.n2);
   const IO* fi = static_cast<const IO*>(a.f_in) + static_cast<size_t>(c) * Q;
   R d[Q];
 #pragma unroll
@@ -508,7 +528,7 @@ __device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
   collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
   for (int q = 0; q < Q; ++q)
-    static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * a.g.ncell + c] = from_r<S>(d[q]);
+    static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * a.g.pstride + ci] = from_r<S>(d[q]);
 }
 
 template <int Q, class S, bool FORCE>
@@ -594,7 +614,8 @@ __device__ __forceinline__ void finish_cell(const StepArgs& a, const Cell& x,
     collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
     for (int q = 0; q < Q; ++q)
-      static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * g.ncell + cidx] = from_r<S>(d[q]);
+      static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * g.pstride + x.srow + x.k] =
+          from_r<S>(d[q]);
   }
 }
 
@@ -604,23 +625,23 @@ __device__ __forceinline__ void pull_cell(const StepArgs& a, const Cell& x,
                                           typename StoreT<S>::R (&d)[Q]) {
   const Geo& g = a.g;
   // Offsets of the source rows of the pull x - e_q (periodic on every axis).
-  const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
-  const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
-  const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.n2 : 0u - g.n2;  // i1 - 1
-  const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.n2 : g.n2;
+  const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.splane : 0u - g.splane;  // i0 - 1
+  const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.splane : g.splane;
+  const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.rstride : 0u - g.rstride;  // i1 - 1
+  const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.rstride : g.rstride;
   const uint32_t km = x.k == 0 ? g.n2 - 1 : x.k - 1;
   const uint32_t kp = x.k == g.n2 - 1 ? 0 : x.k + 1;
 
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
-    uint32_t off = x.row;
+    uint32_t off = x.srow;
     if (c0 > 0) off += dm0;
     if (c0 < 0) off += dp0;
     if (c1 > 0) off += dm1;
     if (c1 < 0) off += dp1;
     off += c2 > 0 ? km : (c2 < 0 ? kp : x.k);
-    d[q] = ld_pop<S>(static_cast<const S*>(a.pin) + (static_cast<uint32_t>(q) * g.ncell + off));
+    d[q] = ld_pop<S>(static_cast<const S*>(a.pin) + (static_cast<uint32_t>(q) * g.pstride + off));
   }
 }
 
@@ -725,7 +746,7 @@ __device__ __forceinline__ void step_cell_any(const StepArgs& a, uint32_t c) {
 // otherwise all members share the one given at compile time (SPEC = 1 +
 // 2 FACES + FORCE), which keeps a single copy of the step body in the kernel.
 template <int Q, class S, int MODE, int SPEC>
-__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+__global__ void __launch_bounds__(kBlock, batched_min_blocks<S>())
     k_batched_step(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                    uint32_t ntiles, int which) {
 #if LBM_BATCH_ARGS_SMEM
@@ -755,7 +776,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
 }
 
 template <int Q, class S>
-__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+__global__ void __launch_bounds__(kBlock, batched_min_blocks<S>())
     k_batched_prepare(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                       uint32_t ntiles) {
   __shared__ StepArgs sa;

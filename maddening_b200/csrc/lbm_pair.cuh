@@ -92,32 +92,42 @@ struct PairT<float> {
 // Resident warps per SM the register budget is set for.
 constexpr int kPairMinWarps = LBM_PAIR_MIN_WARPS;
 
-// Moments and collide of one cell whose f_bc populations are in d.
+// Moments and collide of one cell whose f_bc populations are in d; `real` =
+// false for the padding cell of a padded row (its result is never read).
 template <int Q, class S, bool FORCE>
-__device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, float (&d)[Q]) {
+__device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, float (&d)[Q],
+                                          bool real = true) {
   using IO = typename StoreT<S>::IO;
   float F[3] = {0, 0, 0};
   if (FORCE) {
-    if (a.force_mode == 2) load_force<Q, IO>(a.force_field, x.c, F);
-    else uniform_force<Q, float>(a, F);
+    if (a.force_mode == 2) {
+      if (real) load_force<Q, IO>(a.force_field, x.c, F);
+    } else {
+      uniform_force<Q, float>(a, F);
+    }
   }
   const Mom<float> m = moments<Q, float, FORCE>(d, F);
   collide<Q, float, FORCE>(d, m, F, static_cast<float>(a.omega), static_cast<float>(a.guo_c));
 }
 
 // Everything after the plane loads of one thread's pair (k, k+1) of row
-// `rbase`: v[q] the pair word at (k, k+1) of the source row of direction q,
-// e[q] the word of the pair before (c2 > 0: cell k pulls k - 1) or after
-// (c2 < 0: cell k + 1 pulls k + 2), periodic along the row.  All 32 lanes of
-// the warp must call it (vote); `store` = false for lanes that only pad the
-// warp.
-template <int Q, class S, bool FACES, bool FORCE>
+// `rbase` (reference layout; `sbase` in the state planes): v[q] the pair word
+// at (k, k+1) of the source row of direction q, e[q] the word of the pair
+// before (c2 > 0: cell k pulls k - 1) or after (c2 < 0: cell k + 1 pulls
+// k + 2), periodic along the row.  In a padded row (odd n2, state rows of
+// n2 + 1) the last pair is (n2 - 1, padding): cell 0 finds n2 - 1 and cell
+// n2 - 1 finds 0 in the LOW half of their neighbour word.  All 32 lanes of the
+// warp must call it (vote); `store` = false for lanes that only pad the warp.
+// PAD: the state rows are padded (compile time: the checks cost instructions).
+template <int Q, class S, bool FACES, bool FORCE, bool PAD>
 __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint32_t i1,
-                                            uint32_t k, uint32_t rbase,
+                                            uint32_t k, uint32_t rbase, uint32_t sbase,
                                             const typename PairT<S>::P (&v)[Q],
                                             const typename PairT<S>::P (&e)[Q], bool store) {
   using PT = PairT<S>;
   const Geo& g = a.g;
+  const bool first = PAD && k == 0;
+  const bool last = PAD && k + 1 == g.n2;  // cell b is the padding cell
   float da[Q], db[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
@@ -126,18 +136,23 @@ __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint
       da[q] = PT::lo(v[q]);
       db[q] = PT::hi(v[q]);
     } else if (c2 > 0) {
-      da[q] = PT::hi(e[q]);
+      da[q] = first ? PT::lo(e[q]) : PT::hi(e[q]);
       db[q] = PT::lo(v[q]);
     } else {
-      da[q] = PT::hi(v[q]);
+      da[q] = last ? PT::lo(e[q]) : PT::hi(v[q]);
       db[q] = PT::lo(e[q]);
     }
   }
   bool wa = false, wb = false;
   if (a.wall != nullptr) {
-    const uint32_t w2 = __ldg(reinterpret_cast<const unsigned short*>(a.wall + rbase + k));
-    wa = (w2 & 0xffu) != 0;
-    wb = (w2 >> 8) != 0;
+    if constexpr (PAD) {  // odd rows: the two wall bytes are not 2-byte aligned
+      wa = __ldg(a.wall + rbase + k) != 0;
+      wb = !last && __ldg(a.wall + rbase + k + 1) != 0;
+    } else {
+      const uint32_t w2 = __ldg(reinterpret_cast<const unsigned short*>(a.wall + rbase + k));
+      wa = (w2 & 0xffu) != 0;
+      wb = (w2 >> 8) != 0;
+    }
   }
   Cell xa, xb;
   xa.c = rbase + k;
@@ -145,6 +160,7 @@ __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint
   xa.i1 = i1;
   xa.k = k;
   xa.row = rbase;
+  xa.srow = sbase;
   xb = xa;
   xb.c = xa.c + 1;
   xb.k = k + 1;
@@ -168,16 +184,16 @@ __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint
     }
     if (near) {
       if (!wa) apply_faces<Q, S>(a, xa, da);
-      if (!wb) apply_faces<Q, S>(a, xb, db);
+      if (!wb && !last) apply_faces<Q, S>(a, xb, db);  // never on the padding cell
     }
   }
   pair_cell<Q, S, FORCE>(a, xa, da);
-  pair_cell<Q, S, FORCE>(a, xb, db);
+  pair_cell<Q, S, FORCE>(a, xb, db, !last);
   if (!store) return;
   S* pout = static_cast<S*>(a.pout);
 #pragma unroll
   for (int q = 0; q < Q; ++q)
-    PT::st(pout + (static_cast<uint32_t>(q) * g.ncell + rbase + k), da[q], db[q]);
+    PT::st(pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k), da[q], db[q]);
 }
 
 // Row-segment form: rows of 64 W cells or a multiple (see the header comment).
@@ -206,60 +222,65 @@ __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
     const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
     const uint32_t s0 = c0 > 0 ? i0m : (c0 < 0 ? i0p : i0);
     const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
-    const S* base = pin + (static_cast<uint32_t>(q) * g.ncell + (s0 * g.n1 + s1) * g.n2);
+    const S* base = pin + (static_cast<uint32_t>(q) * g.pstride + (s0 * g.n1 + s1) * g.rstride);
     v[q] = PT::ld(base + k);
     if (c2 > 0) e[q] = PT::ld(base + kprev);
     if (c2 < 0) e[q] = PT::ld(base + knext);
   }
-  pair_finish<Q, S, FACES, FORCE>(a, i0, i1, k, row * g.n2, v, e, true);
+  pair_finish<Q, S, FACES, FORCE, false>(a, i0, i1, k, row * g.n2, row * g.rstride, v, e, true);
 }
 
-// Pairs of one instance-wide index: pair j holds cells 2j, 2j + 1 (rows of even
-// length, so a pair never spans two rows).  Row coordinates and source rows
-// are per lane.
-template <int Q, class S, bool FACES, bool FORCE>
+// Pairs of the state planes' index: pair j holds state cells 2j, 2j + 1 (rows
+// of even length -- padded ones included -- so a pair never spans two rows).
+// Row coordinates and source rows are per lane.  PAD: padded state rows.
+template <int Q, class S, bool FACES, bool FORCE, bool PAD>
 __device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
   using PT = PairT<S>;
   using P = typename PT::P;
   const Geo& g = a.g;
-  const uint32_t npairs = g.ncell >> 1;
+  const uint32_t npairs = g.pstride >> 1;
   const bool valid = pidx < npairs;
-  const Cell x = locate(g, 2u * (valid ? pidx : npairs - 1u));
-  const uint32_t dm0 = x.i0 == 0 ? (g.n0 - 1) * g.plane : 0u - g.plane;  // i0 - 1
-  const uint32_t dp0 = x.i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.plane : g.plane;
-  const uint32_t dm1 = x.i1 == 0 ? (g.n1 - 1) * g.n2 : 0u - g.n2;  // i1 - 1
-  const uint32_t dp1 = x.i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.n2 : g.n2;
-  const uint32_t kprev = (x.k == 0 ? g.n2 : x.k) - 2u;
-  const uint32_t knext = x.k + 2 == g.n2 ? 0u : x.k + 2;
+  const uint32_t ci = 2u * (valid ? pidx : npairs - 1u);
+  const uint32_t r = fdiv(ci, g.div_rstride);  // row index
+  const uint32_t k = ci - r * g.rstride;
+  const uint32_t i0 = fdiv(r, g.div_n1);
+  const uint32_t i1 = r - i0 * g.n1;
+  const uint32_t srow = r * g.rstride;
+  const uint32_t dm0 = i0 == 0 ? (g.n0 - 1) * g.splane : 0u - g.splane;  // i0 - 1
+  const uint32_t dp0 = i0 == g.n0 - 1 ? 0u - (g.n0 - 1) * g.splane : g.splane;
+  const uint32_t dm1 = i1 == 0 ? (g.n1 - 1) * g.rstride : 0u - g.rstride;  // i1 - 1
+  const uint32_t dp1 = i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.rstride : g.rstride;
+  const uint32_t kprev = (k == 0 ? g.rstride : k) - 2u;
+  const uint32_t knext = k + 2 == g.rstride ? 0u : k + 2;
   const S* pin = static_cast<const S*>(a.pin);
   P v[Q];
   P e[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
-    uint32_t off = x.row;
+    uint32_t off = srow;
     if (c0 > 0) off += dm0;
     if (c0 < 0) off += dp0;
     if (c1 > 0) off += dm1;
     if (c1 < 0) off += dp1;
-    const S* base = pin + (static_cast<uint32_t>(q) * g.ncell + off);
-    v[q] = PT::ld(base + x.k);
+    const S* base = pin + (static_cast<uint32_t>(q) * g.pstride + off);
+    v[q] = PT::ld(base + k);
     if (c2 > 0) e[q] = PT::ld(base + kprev);
     if (c2 < 0) e[q] = PT::ld(base + knext);
   }
-  pair_finish<Q, S, FACES, FORCE>(a, x.i0, x.i1, x.k, x.row, v, e, valid);
+  pair_finish<Q, S, FACES, FORCE, PAD>(a, i0, i1, k, r * g.n2, srow, v, e, valid);
 }
 
 template <int Q, class S, bool FACES, bool FORCE>
 __global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
     k_step_gpair(const __grid_constant__ StepArgs a) {
-  gpair_step<Q, S, FACES, FORCE>(a, blockIdx.x * kBlock + threadIdx.x);
+  gpair_step<Q, S, FACES, FORCE, false>(a, blockIdx.x * kBlock + threadIdx.x);
 }
 
 // Batched ensemble, state steps of members with even rows: a tile of
 // kBatchTile cells is kBatchTile / 2 pairs, kBatchTile / (2 kBlock) per thread
 // (see k_batched_step for the tile walk and SPEC).
-template <int Q, class S, int SPEC>
+template <int Q, class S, int SPEC, bool PAD>
 __global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
     k_batched_pair(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                    uint32_t ntiles, int which) {
@@ -284,19 +305,19 @@ __global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
       const uint32_t pidx = (tile.first >> 1) + j * kBlock + threadIdx.x;
       // whole warps past the member's last pair skip the step; a partial warp
       // runs it with its extra lanes clamped
-      if ((((tile.first >> 1) + j * kBlock + (threadIdx.x & ~31u)) << 1) >= sa.g.ncell) break;
+      if ((((tile.first >> 1) + j * kBlock + (threadIdx.x & ~31u)) << 1) >= sa.g.pstride) break;
       if constexpr (SPEC == 0) {
         const bool faces = sa.face[0].kind != kFaceNone || sa.face[1].kind != kFaceNone;
         const bool force = sa.force_mode != 0;
         if (faces) {
-          if (force) gpair_step<Q, S, true, true>(sa, pidx);
-          else gpair_step<Q, S, true, false>(sa, pidx);
+          if (force) gpair_step<Q, S, true, true, PAD>(sa, pidx);
+          else gpair_step<Q, S, true, false, PAD>(sa, pidx);
         } else {
-          if (force) gpair_step<Q, S, false, true>(sa, pidx);
-          else gpair_step<Q, S, false, false>(sa, pidx);
+          if (force) gpair_step<Q, S, false, true, PAD>(sa, pidx);
+          else gpair_step<Q, S, false, false, PAD>(sa, pidx);
         }
       } else {
-        gpair_step<Q, S, ((SPEC - 1) & 2) != 0, ((SPEC - 1) & 1) != 0>(sa, pidx);
+        gpair_step<Q, S, ((SPEC - 1) & 2) != 0, ((SPEC - 1) & 1) != 0, PAD>(sa, pidx);
       }
     }
   }

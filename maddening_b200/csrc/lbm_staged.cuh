@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(T, staged_min_blocks<S, T>())
       const uint32_t j0 = c0 > 0 ? r0m : (c0 < 0 ? r0p : i0);
       const uint32_t j1 = c1 > 0 ? r1m : (c1 < 0 ? r1p : i1);
       const S* src = static_cast<const S*>(a.pin) +
-                     (static_cast<uint32_t>(q) * g.ncell + (j0 * g.n1 + j1) * g.n2);
+                     (static_cast<uint32_t>(q) * g.pstride + (j0 * g.n1 + j1) * g.rstride);
       bulk_copy_g2s(dst + static_cast<size_t>(q) * row_bytes, src, row_bytes, &bars[s]);
     }
   };
@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(T, staged_min_blocks<S, T>())
     x.i0 = fdiv(row, g.div_n1);
     x.i1 = row - x.i0 * g.n1;
     x.row = row * g.n2;
+    x.srow = row * g.rstride;
     for (uint32_t k = threadIdx.x; k < g.n2; k += T) {
       x.k = k;
       x.c = x.row + k;

@@ -18,9 +18,10 @@ def _members(storage="f32", lattice="D3Q19"):
     from maddening_b200 import LBMNode
     rng = np.random.default_rng(21)
     if lattice == "D3Q19":
-        shapes = [(9, 7, 13), (16, 16, 16), (5, 12, 33), (20, 8, 6), (3, 4, 130), (11, 10, 9)]
+        shapes = [(9, 7, 13), (16, 16, 16), (5, 12, 33), (20, 8, 6), (3, 4, 130), (11, 10, 9),
+                  (4, 6, 15)]
     else:
-        shapes = [(17, 9), (40, 33), (6, 131), (25, 4), (12, 12)]
+        shapes = [(17, 9), (40, 33), (6, 131), (25, 4), (12, 12), (7, 13)]
     nodes, bis, states = [], [], []
     for i, shape in enumerate(shapes):
         tau = float(rng.uniform(0.55, 1.5))
@@ -38,6 +39,14 @@ def _members(storage="f32", lattice="D3Q19"):
             bi = {"inlet_velocity": np.array([0.03] + [0.0] * (len(shape) - 1))}
         if i == 3:
             bi["body_force"] = rng.uniform(-1e-5, 1e-5, shape + (len(shape),)).astype(np.float32)
+        if i == len(shapes) - 1:
+            # faces on the contiguous axis of an odd row (padded state rows)
+            ax = "z" if len(shape) == 3 else "y"
+            kw = dict(inlet_face=f"{ax}_min", outlet_face=f"{ax}_max",
+                      outlet_condition="zero_gradient")
+            wall[..., 0] = wall[..., -1] = False
+            bi = {"inlet_velocity": np.array([0.0] * (len(shape) - 1) + [0.02]),
+                  "body_force": rng.uniform(-1e-5, 1e-5, shape + (len(shape),)).astype(np.float32)}
         node = LBMNode(f"m{i}", 1.0, grid_shape=shape, viscosity=(tau - 0.5) / 3.0,
                        lattice=lattice, wall_mask=wall, storage=storage, **kw)
         st = node.initial_state()
@@ -57,7 +66,7 @@ CONFIGS = [{"blocks_per_sm": b, "tile_order": o, "use_graph": g, "group_mib": m}
 
 
 @pytest.mark.parametrize("lattice", ["D3Q19", "D2Q9"])
-@pytest.mark.parametrize("storage", ["f32", "f16", "f64"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
 def test_batched_members_equal_their_own_rollouts(lattice, storage):
     from maddening_b200.batched import LBMEnsemble
     nodes, bis, states = _members(storage, lattice)
