@@ -177,6 +177,27 @@ int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
                 void* f_out, int64_t n_steps, const lbm_step_args* args,
                 const lbm_moments* out, void* workspace, size_t workspace_bytes);
 
+/* History of a rollout, GraphManager.run_scan_with_history
+ * (graph_manager.py:2753-2805), which stacks the whole state after every step.
+ * Record r holds the reference state after step (r + 1) * every, for
+ * r < n_steps / every; each pointer (NULL = field not recorded) points at
+ * n_steps / every consecutive arrays: f (*grid_shape, Q), density grid_shape,
+ * velocity (*grid_shape, D) (0 in walls), pressure grid_shape. */
+typedef struct {
+  void* f;
+  void* density;
+  void* velocity;
+  void* pressure;
+} lbm_history;
+
+/* lbm_rollout that also fills `history`; recorded steps write their outputs
+ * while they collide, the others run as in lbm_rollout (same results bit for
+ * bit).  Workspace: lbm_workspace_bytes. */
+int lbm_rollout_history(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+                        void* f_out, int64_t n_steps, int64_t every,
+                        const lbm_step_args* args, const lbm_moments* out,
+                        const lbm_history* history, void* workspace, size_t workspace_bytes);
+
 /* ---- Differentiated rollout --------------------------------------------
  * Reverse mode of lbm_rollout for walls and body forces (no face conditions),
  * FP32 or FP64 storage.  The reference differentiates LBMNode.update with

@@ -61,6 +61,11 @@ class lbm_moments(C.Structure):
                 ("pressure", C.c_void_p), ("flags", C.c_uint32)]
 
 
+class lbm_history(C.Structure):
+    _fields_ = [("f", C.c_void_p), ("density", C.c_void_p), ("velocity", C.c_void_p),
+                ("pressure", C.c_void_p)]
+
+
 _P = C.c_void_p
 _SIGS = {
     "lbm_abi_version": ([], C.c_int),
@@ -78,6 +83,9 @@ _SIGS = {
                             C.POINTER(lbm_moments)], C.c_int),
     "lbm_update_padded": ([_P, _P, _P, _P, C.POINTER(lbm_step_args), C.POINTER(lbm_moments),
                            _P, C.c_size_t], C.c_int),
+    "lbm_rollout_history": ([_P, _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(lbm_step_args),
+                             C.POINTER(lbm_moments), C.POINTER(lbm_history), _P, C.c_size_t],
+                            C.c_int),
     "lbm_adjoint_workspace_bytes": ([_P, C.c_int64, C.c_int64, C.POINTER(C.c_size_t)],
                                     C.c_int),
     "lbm_rollout_forward": ([_P, _P, _P, _P, C.c_int64, C.c_int64, C.POINTER(lbm_step_args),

@@ -372,6 +372,72 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   return launch_step<Q, S>(a, true, s);
 }
 
+// Rollout that also records the reference state after every `every`-th step
+// (record r = after step (r + 1) every): recorded state steps write f and the
+// moments into the history slots as they collide; the last step's outputs are
+// copied into its slot when it is recorded.
+template <int Q, class S>
+int run_history(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in,
+                void* f_out, int64_t n, int64_t every, const lbm_history* h, char* ws) {
+  const size_t sb = align256(state_bytes(p));
+  const size_t cells = p->g.ncell;
+  const size_t fb = cells * p->Q * p->io, rb = cells * p->io, vb = cells * p->D * p->io;
+  auto slot = [](void* base, size_t bytes, int64_t r) -> void* {
+    return base == nullptr ? nullptr : static_cast<char*>(base) + static_cast<size_t>(r) * bytes;
+  };
+  char* A = ws;
+  char* B = ws + sb;
+  lbm::StepArgs m = a;
+  m.rho = m.vel = m.prs = nullptr;
+  m.f_in = f_in;
+  m.pout = A;
+  int rc = launch_prepare<Q, S>(m, s);
+  if (rc) return rc;
+  for (int64_t i = 1; i < n; ++i) {
+    m.pin = A;
+    m.pout = B;
+    if (i % every == 0) {
+      const int64_t r = i / every - 1;
+      lbm::StepArgs rec = m;
+      rec.f_out = slot(h->f, fb, r);
+      rec.rho = slot(h->density, rb, r);
+      rec.vel = slot(h->velocity, vb, r);
+      rec.prs = slot(h->pressure, rb, r);
+      launch_step_mode<Q, S, lbm::kOutRecord>(rec, s);
+      rc = cuda_check(cudaGetLastError(), "k_step launch");
+    } else {
+      rc = launch_state_step<Q, S>(p, m, s);
+    }
+    if (rc) return rc;
+    char* t = A;
+    A = B;
+    B = t;
+  }
+  const bool last = n % every == 0;
+  const int64_t r = n / every - 1;
+  a.pin = A;
+  a.f_out = f_out;
+  // the last step's moments go to the caller's buffers, or straight to the
+  // history slot when the caller wants none
+  if (last && a.rho == nullptr) a.rho = slot(h->density, rb, r);
+  if (last && a.vel == nullptr) a.vel = slot(h->velocity, vb, r);
+  if (last && a.prs == nullptr) a.prs = slot(h->pressure, rb, r);
+  rc = launch_step<Q, S>(a, true, s);
+  if (rc || !last) return rc;
+  struct { void* dst; const void* src; size_t bytes; } copies[4] = {
+      {slot(h->f, fb, r), f_out, fb},
+      {slot(h->density, rb, r), a.rho, rb},
+      {slot(h->velocity, vb, r), a.vel, vb},
+      {slot(h->pressure, rb, r), a.prs, rb}};
+  for (const auto& c : copies) {
+    if (c.dst == nullptr || c.dst == c.src) continue;
+    rc = cuda_check(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice, s),
+                    "cudaMemcpyAsync");
+    if (rc) return rc;
+  }
+  return LBM_OK;
+}
+
 template <int Q>
 int dispatch_s(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a, const void* f_in,
                void* f_out, int64_t n, char* ws) {
@@ -869,6 +935,42 @@ int lbm_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, voi
                 void* workspace, size_t workspace_bytes) {
   return do_steps(plan, stream, f_in, f_out, n_steps, args, out, workspace, workspace_bytes,
                   n_steps > 1 ? 2 : 1);
+}
+
+int lbm_rollout_history(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* f_out,
+                        int64_t n_steps, int64_t every, const lbm_step_args* args,
+                        const lbm_moments* out, const lbm_history* history, void* workspace,
+                        size_t workspace_bytes) {
+  if (p == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
+  if (f_in == nullptr || f_out == nullptr) return fail(LBM_ERR_INVALID, "f_in/f_out is NULL");
+  if (history == nullptr) return fail(LBM_ERR_INVALID, "history is NULL");
+  if (n_steps < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)n_steps);
+  if (every < 1) return fail(LBM_ERR_INVALID, "every must be >= 1 (got %lld)", (long long)every);
+  const size_t need = 2 * align256(state_bytes(p)) + 256;
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", need,
+                workspace_bytes);
+  lbm::StepArgs a;
+  int rc = build_args(p, args, out, &a);
+  if (rc) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  if (p->Q == 19) {
+    switch (p->storage) {
+      case LBM_STORE_F32: return run_history<19, float>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+      case LBM_STORE_F16: return run_history<19, __half>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+      case LBM_STORE_BF16: return run_history<19, __nv_bfloat16>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+      case LBM_STORE_F64: return run_history<19, double>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+    }
+  } else {
+    switch (p->storage) {
+      case LBM_STORE_F32: return run_history<9, float>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+      case LBM_STORE_F16: return run_history<9, __half>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+      case LBM_STORE_BF16: return run_history<9, __nv_bfloat16>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+      case LBM_STORE_F64: return run_history<9, double>(p, s, a, f_in, f_out, n_steps, every, history, ws);
+    }
+  }
+  return fail(LBM_ERR_INVALID, "bad storage");
 }
 
 int lbm_update_padded(const lbm_plan* p, lbm_stream_t stream, const void* f_pad,

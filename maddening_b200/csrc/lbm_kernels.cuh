@@ -440,7 +440,10 @@ constexpr int min_blocks() { return sizeof(typename StoreT<S>::R) == 8 ? kMinBlo
 template <class S>
 constexpr int batched_min_blocks() { return sizeof(typename StoreT<S>::R) == 8 ? 4 : 8; }
 
-enum StepMode : int { kOutState = 0, kOutAoS = 1, kOutMoments = 2 };
+// kOutState: the next state; kOutAoS: the reference f (last step); kOutMoments:
+// moments only; kOutRecord: the next state and, where the pointers are set,
+// the reference f and the moments of this step (a recorded history step).
+enum StepMode : int { kOutState = 0, kOutAoS = 1, kOutMoments = 2, kOutRecord = 3 };
 
 struct Cell {
   uint32_t c;      // linear cell index (reference layout)
@@ -606,11 +609,14 @@ __device__ __forceinline__ void finish_cell(const StepArgs& a, const Cell& x,
   const Mom<R> m = moments<Q, R, FORCE>(d, F);
   store_moments<Q, IO>(a, cidx, m, wall);
 
-  if constexpr (MODE == kOutAoS) {
-    IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(cidx) * Q;
+  if constexpr (MODE == kOutAoS || MODE == kOutRecord) {
+    if (MODE == kOutAoS || a.f_out != nullptr) {
+      IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(cidx) * Q;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) fo[q] = static_cast<IO>(from_offset<Q, R>(d[q], q));
-  } else if constexpr (MODE == kOutState) {
+      for (int q = 0; q < Q; ++q) fo[q] = static_cast<IO>(from_offset<Q, R>(d[q], q));
+    }
+  }
+  if constexpr (MODE == kOutState || MODE == kOutRecord) {
     collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
     for (int q = 0; q < Q; ++q)

@@ -11,6 +11,9 @@ Additions beyond the reference (documented extensions):
 
 * ``run(state, boundary_inputs, n_steps)`` -- ``n_steps`` reference steps in
   one call, populations kept on the device as offsets between steps.
+* ``run_with_history(state, boundary_inputs, n_steps, every=, fields=)`` -- the
+  same, also returning the stacked state after every ``every``-th step (the
+  node's part of ``run_scan_with_history``).
 * boundary input ``inlet_velocity`` (D,) -- velocity face at ``inlet_face``.
 * ``outlet_condition="zero_gradient"`` -- zero-gradient face at
   ``outlet_face`` on every step.
@@ -364,6 +367,48 @@ class LBMNode(SimulationNode):
         if "wall_mask" in state:
             out["wall_mask"] = state["wall_mask"]
         return out
+
+    def run_with_history(self, state: dict, boundary_inputs: dict, n_steps: int, *,
+                         every: int = 1,
+                         fields=("f", "density", "velocity", "pressure")):
+        """``n_steps`` fused steps that also return the state after every
+        ``every``-th step -- the node's share of ``GraphManager.
+        run_scan_with_history`` (graph_manager.py:2753-2805), which stacks the
+        whole state after each step.  Returns ``(final_state, history)`` with
+        ``history[key]`` of shape ``(n_steps // every, *field_shape)`` for each
+        key of ``fields`` (``f`` is 76 bytes per cell and record: leave it out,
+        or record sparsely, for long rollouts).  The records equal the outputs
+        of ``run`` with that many steps, bit for bit."""
+        n = int(n_steps)
+        every = int(every)
+        if n < 1 or every < 1:
+            raise ValueError("n_steps and every must be >= 1")
+        fields = tuple(fields)
+        bad = set(fields) - {"f", "density", "velocity", "pressure"}
+        if bad:
+            raise ValueError(f"unknown history fields {sorted(bad)}")
+        dev = self._dev()
+        f_in = self._f_in(state, dev)
+        args, keep = self._step_args(state, boundary_inputs or {}, dev)
+        f, rho, vel, prs, m = self._outputs(dev)
+        nrec = n // every
+        shapes = {"f": self._grid_shape + (self._Q,), "density": self._grid_shape,
+                  "velocity": self._grid_shape + (self._D,), "pressure": self._grid_shape}
+        history = {k: torch.empty((nrec,) + shapes[k], dtype=self._io_dtype, device=dev)
+                   for k in fields}
+        h = _lib.lbm_history()
+        for k, t in history.items():
+            setattr(h, k, t.data_ptr() if nrec > 0 else None)
+        ws = torch.empty(self._plan.workspace_bytes(), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_rollout_history(
+            self._plan.handle, stream, f_in.data_ptr(), f.data_ptr(), n, every, C.byref(args),
+            C.byref(m), C.byref(h), ws.data_ptr(), ws.numel()))
+        del keep
+        out = {"f": f, "density": rho, "velocity": vel, "pressure": prs}
+        if "wall_mask" in state:
+            out["wall_mask"] = state["wall_mask"]
+        return out, history
 
     def update(self, state: dict, boundary_inputs: dict, dt: float) -> dict:
         """One reference step (lbm.py:899-986)."""
