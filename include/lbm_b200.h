@@ -198,6 +198,34 @@ int lbm_rollout_history(const lbm_plan* plan, lbm_stream_t stream, const void* f
                         const lbm_step_args* args, const lbm_moments* out,
                         const lbm_history* history, void* workspace, size_t workspace_bytes);
 
+/* ---- Pipe node -----------------------------------------------------------
+ * MADDENING's LBMPipeNode (src/maddening/nodes/lbm_pipe.py:393-879), single
+ * phase: D3Q19 BGK with the Guo source of an actuator-disc propeller (x force
+ * on the disc cells of plane propeller_x) and gravity (z force on every
+ * non-wall cell), moments without the half-force step, periodic stream,
+ * wall-node swap; then the D3Q7 passive tracer collided with the step's new
+ * velocity (not in walls), streamed and wall-swapped.  The plan is D3Q19 with
+ * FP32 or FP64 storage. */
+typedef struct {
+  const uint8_t* wall;       /* grid, nonzero = wall                                */
+  const uint8_t* propeller;  /* (ny, nz) disc mask of the propeller plane, or NULL */
+  int32_t propeller_x;       /* the propeller plane (x index)                      */
+  double propeller_force;    /* x force on the disc cells                          */
+  double gravity;            /* z force on the non-wall cells                      */
+  double tau_tracer;         /* tracer relaxation time, > 0.5                      */
+} lbm_pipe_args;
+
+int lbm_pipe_workspace_bytes(const lbm_plan* plan, size_t* bytes);
+
+/* n_steps pipe-node steps.  f: (*grid, 19); tracer_f: (*grid, 7); outputs of
+ * the last step: f_out, tracer_f_out, out->density / out->velocity (0 in
+ * walls; out->pressure is not written), tracer_out (grid, 0 in walls; NULL =
+ * not written).  Inputs may not alias outputs. */
+int lbm_pipe_rollout(const lbm_plan* plan, lbm_stream_t stream, const void* f_in, void* f_out,
+                     const void* tracer_f_in, void* tracer_f_out, int64_t n_steps,
+                     const lbm_pipe_args* args, const lbm_moments* out, void* tracer_out,
+                     void* workspace, size_t workspace_bytes);
+
 /* ---- Differentiated rollout --------------------------------------------
  * Reverse mode of lbm_rollout for walls and body forces (no face conditions),
  * FP32 or FP64 storage.  The reference differentiates LBMNode.update with

@@ -15,6 +15,7 @@
 #include "lbm_adjoint.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_pair.cuh"
+#include "lbm_pipe.cuh"
 #include "lbm_staged.cuh"
 
 struct lbm_plan {
@@ -971,6 +972,130 @@ int lbm_rollout_history(const lbm_plan* p, lbm_stream_t stream, const void* f_in
     }
   }
   return fail(LBM_ERR_INVALID, "bad storage");
+}
+
+}  // extern "C"
+
+namespace {
+
+size_t pipe_workspace(const lbm_plan* p) {
+  const size_t n = p->g.ncell;
+  return 2 * align256(state_bytes(p)) + 2 * align256(7 * n * p->io) + align256(3 * n * p->io);
+}
+
+template <class S>
+int run_pipe(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
+             const void* t_in, void* t_out, int64_t n, double tau_tracer, void* tracer_out,
+             char* ws) {
+  using IO = typename lbm::StoreT<S>::IO;
+  const size_t cells = p->g.ncell;
+  const size_t sb = align256(state_bytes(p)), tb = align256(7 * cells * p->io);
+  char* A = ws;
+  char* B = ws + sb;
+  char* T[2] = {ws + 2 * sb, ws + 2 * sb + tb};
+  char* U = ws + 2 * sb + 2 * tb;
+  const unsigned grid = grid_for(p->g.ncell);
+  lbm::TracerArgs t{};
+  t.g = p->g;
+  t.wall = a.wall;
+  t.inv_tau = 1.0 / tau_tracer;
+  t.f7_in = t_in;
+  t.tout = T[0];
+  lbm::k_tracer_prepare<IO><<<grid, lbm::kBlock, 0, s>>>(t);
+  int rc = cuda_check(cudaGetLastError(), "k_tracer_prepare launch");
+  if (rc) return rc;
+  lbm::StepArgs m = a;
+  m.rho = m.prs = m.vel = nullptr;
+  m.f_in = f_in;
+  m.pout = A;
+  rc = launch_prepare<19, S>(m, s);
+  if (rc) return rc;
+  int cur = 0;
+  auto tracer_step = [&](const void* vel) {
+    t.tin = T[cur];
+    t.tout = T[1 - cur];
+    t.vel = vel;
+    lbm::k_tracer_step<IO><<<grid, lbm::kBlock, 0, s>>>(t);
+    cur = 1 - cur;
+    return cuda_check(cudaGetLastError(), "k_tracer_step launch");
+  };
+  m.vel = U;  // each step's velocity (0 in walls) for the tracer
+  m.mflags = 0;
+  for (int64_t i = 1; i < n; ++i) {
+    m.pin = A;
+    m.pout = B;
+    rc = launch_step<19, S>(m, false, s);
+    if (rc) return rc;
+    rc = tracer_step(U);
+    if (rc) return rc;
+    char* x = A;
+    A = B;
+    B = x;
+  }
+  a.pin = A;
+  a.f_out = f_out;
+  a.prs = nullptr;
+  a.mflags &= ~lbm::kMomRawVelocity;
+  if (a.vel == nullptr) a.vel = U;
+  rc = launch_step<19, S>(a, true, s);
+  if (rc) return rc;
+  rc = tracer_step(a.vel);
+  if (rc) return rc;
+  t.tin = T[cur];
+  t.f7_out = t_out;
+  t.tracer_out = tracer_out;
+  lbm::k_tracer_final<IO><<<grid, lbm::kBlock, 0, s>>>(t);
+  return cuda_check(cudaGetLastError(), "k_tracer_final launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_pipe_workspace_bytes(const lbm_plan* plan, size_t* bytes) {
+  if (plan == nullptr || bytes == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  *bytes = pipe_workspace(plan);
+  return LBM_OK;
+}
+
+int lbm_pipe_rollout(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* f_out,
+                     const void* tracer_f_in, void* tracer_f_out, int64_t n_steps,
+                     const lbm_pipe_args* pa, const lbm_moments* out, void* tracer_out,
+                     void* workspace, size_t workspace_bytes) {
+  if (p == nullptr || pa == nullptr) return fail(LBM_ERR_INVALID, "NULL argument");
+  if (p->Q != 19) return fail(LBM_ERR_UNSUPPORTED, "the pipe node is D3Q19");
+  if (p->storage != LBM_STORE_F32 && p->storage != LBM_STORE_F64)
+    return fail(LBM_ERR_UNSUPPORTED, "the pipe node runs FP32 or FP64 storage");
+  if (f_in == nullptr || f_out == nullptr || tracer_f_in == nullptr || tracer_f_out == nullptr)
+    return fail(LBM_ERR_INVALID, "f / tracer_f is NULL");
+  if (n_steps < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)n_steps);
+  if (!(pa->tau_tracer > 0.5)) return fail(LBM_ERR_INVALID, "tau_tracer must be > 0.5");
+  if (pa->propeller != nullptr &&
+      (pa->propeller_x < 0 || pa->propeller_x >= static_cast<int32_t>(p->g.n0)))
+    return fail(LBM_ERR_INVALID, "propeller_x %d outside [0, %u)", pa->propeller_x, p->g.n0);
+  const size_t need = pipe_workspace(p);
+  if (workspace == nullptr || workspace_bytes < need)
+    return fail(LBM_ERR_WORKSPACE, "workspace of %zu bytes needed, %zu given", need,
+                workspace_bytes);
+  lbm_step_args sa{};
+  sa.force_mode = LBM_FORCE_NONE;
+  sa.wall = pa->wall;
+  lbm::StepArgs a;
+  int rc = build_args(p, &sa, out, &a);
+  if (rc) return rc;
+  a.force_mode = 3;
+  a.force[0] = pa->propeller != nullptr ? pa->propeller_force : 0.0;
+  a.force[1] = 0.0;
+  a.force[2] = pa->gravity;
+  a.prop_x = pa->propeller != nullptr ? static_cast<uint32_t>(pa->propeller_x) : 0xffffffffu;
+  a.prop_mask = pa->propeller;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  if (p->storage == LBM_STORE_F32)
+    return run_pipe<float>(p, s, a, f_in, f_out, tracer_f_in, tracer_f_out, n_steps,
+                           pa->tau_tracer, tracer_out, ws);
+  return run_pipe<double>(p, s, a, f_in, f_out, tracer_f_in, tracer_f_out, n_steps,
+                          pa->tau_tracer, tracer_out, ws);
 }
 
 int lbm_update_padded(const lbm_plan* p, lbm_stream_t stream, const void* f_pad,

@@ -135,6 +135,11 @@ struct StepArgs {
   // Face planes sit this many cells inside the lattice: 0, or 1 for a
   // halo-padded block (the faces act on the interior).
   uint32_t face_inset;
+  // force_mode 3 (the pipe node): x force force[0] on the cells of plane i0 =
+  // prop_x where prop_mask[i1 n2 + k] is set, z force force[2] on every
+  // non-wall cell; moments without the half-force step.
+  uint32_t prop_x;
+  const uint8_t* prop_mask;
 };
 
 constexpr uint32_t kMomDensityDev = 1u;
@@ -223,7 +228,7 @@ struct Mom {
 // rollout (FP32: 1.3e-5 relative L2 of u after 500 steps of the 64^3 channel,
 // against 2.9e-6 with exact weights).
 template <int Q, class R, bool FORCE = true>
-__device__ __forceinline__ Mom<R> moments(const R (&d)[Q], const R (&F)[3]) {
+__device__ __forceinline__ Mom<R> moments(const R (&d)[Q], const R (&F)[3], bool half = true) {
   constexpr double kDen = Lat<Q>::kWDen;
   R rdp = mul_r(static_cast<R>(Lat<Q>::wr(0)), d[0]);  // 36 (rho - 1)
   R m[3] = {0, 0, 0};                                   // 36 rho u
@@ -246,8 +251,10 @@ __device__ __forceinline__ Mom<R> moments(const R (&d)[Q], const R (&F)[3]) {
     }
   }
   if constexpr (FORCE) {
+    if (half) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) m[k] = fma_r(static_cast<R>(0.5 * kDen), F[k], m[k]);
+      for (int k = 0; k < 3; ++k) m[k] = fma_r(static_cast<R>(0.5 * kDen), F[k], m[k]);
+    }
   }
   // 1/36 = c_hi + c_lo to twice the working precision
   constexpr R c_hi = static_cast<R>(1.0 / kDen);
@@ -464,6 +471,20 @@ __device__ __forceinline__ Cell locate(const Geo& g, uint32_t c) {
   return x;
 }
 
+// Pipe-node force of cell c (force_mode 3, LBMPipeNode.update lbm_pipe.py:766-779).
+template <class R>
+__device__ __forceinline__ void pipe_force(const StepArgs& a, uint32_t c, bool wall, R (&F)[3]) {
+  const Geo& g = a.g;
+  const uint32_t r = fdiv(c, g.div_n2);
+  const uint32_t k = c - r * g.n2;
+  const uint32_t i0 = fdiv(r, g.div_n1);
+  const uint32_t i1 = r - i0 * g.n1;
+  F[0] = (i0 == a.prop_x && __ldg(a.prop_mask + i1 * g.n2 + k) != 0) ? static_cast<R>(a.force[0])
+                                                                        : R(0);
+  F[1] = 0;
+  F[2] = wall ? R(0) : static_cast<R>(a.force[2]);
+}
+
 template <int Q, class IO>
 __device__ __forceinline__ void load_force(const void* force_field, uint32_t c,
                                            typename StoreT<IO>::R (&F)[3]) {
@@ -523,9 +544,10 @@ __device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
   R F[3] = {0, 0, 0};
   if (FORCE) {
     if (a.force_mode == 2) load_force<Q, IO>(a.force_field, c, F);
+    else if (a.force_mode == 3) pipe_force<R>(a, c, a.wall != nullptr && a.wall[c] != 0, F);
     else uniform_force<Q, R>(a, F);
   }
-  const Mom<R> m = moments<Q, R, FORCE>(d, F);
+  const Mom<R> m = moments<Q, R, FORCE>(d, F, a.force_mode != 3);
   if (a.rho != nullptr || a.vel != nullptr || a.prs != nullptr)
     store_moments<Q, IO>(a, c, m, a.wall != nullptr && a.wall[c] != 0);
   collide<Q, R, FORCE>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
@@ -603,10 +625,11 @@ __device__ __forceinline__ void finish_cell(const StepArgs& a, const Cell& x,
   R F[3] = {0, 0, 0};
   if (FORCE) {
     if (a.force_mode == 2) load_force<Q, IO>(a.force_field, cidx, F);
+    else if (a.force_mode == 3) pipe_force<R>(a, cidx, wall, F);
     else uniform_force<Q, R>(a, F);
   }
   apply_bc<Q, S, FACES>(a, x, wall, d);
-  const Mom<R> m = moments<Q, R, FORCE>(d, F);
+  const Mom<R> m = moments<Q, R, FORCE>(d, F, a.force_mode != 3);
   store_moments<Q, IO>(a, cidx, m, wall);
 
   if constexpr (MODE == kOutAoS || MODE == kOutRecord) {

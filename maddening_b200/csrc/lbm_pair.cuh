@@ -86,11 +86,17 @@ struct PairT<float> {
   }
 };
 
+// Resident warps per SM the register budgets are set for (a B200 sweep of
+// 20-32: the row-segment form is fastest at 32 warps despite a few spilled
+// registers, the instance-wide form at 28).
 #ifndef LBM_PAIR_MIN_WARPS
-#define LBM_PAIR_MIN_WARPS 24
+#define LBM_PAIR_MIN_WARPS 32
 #endif
-// Resident warps per SM the register budget is set for.
+#ifndef LBM_GPAIR_MIN_WARPS
+#define LBM_GPAIR_MIN_WARPS 28
+#endif
 constexpr int kPairMinWarps = LBM_PAIR_MIN_WARPS;
+constexpr int kGPairMinWarps = LBM_GPAIR_MIN_WARPS;
 
 // Moments and collide of one cell whose f_bc populations are in d; `real` =
 // false for the padding cell of a padded row (its result is never read).
@@ -272,7 +278,7 @@ __device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
 }
 
 template <int Q, class S, bool FACES, bool FORCE>
-__global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
+__global__ void __launch_bounds__(kBlock, kGPairMinWarps / (kBlock / 32))
     k_step_gpair(const __grid_constant__ StepArgs a) {
   gpair_step<Q, S, FACES, FORCE, false>(a, blockIdx.x * kBlock + threadIdx.x);
 }
@@ -281,7 +287,7 @@ __global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
 // kBatchTile cells is kBatchTile / 2 pairs, kBatchTile / (2 kBlock) per thread
 // (see k_batched_step for the tile walk and SPEC).
 template <int Q, class S, int SPEC, bool PAD>
-__global__ void __launch_bounds__(kBlock, kPairMinWarps / (kBlock / 32))
+__global__ void __launch_bounds__(kBlock, kGPairMinWarps / (kBlock / 32))
     k_batched_pair(const StepArgs* __restrict__ args, const BatchTile* __restrict__ tiles,
                    uint32_t ntiles, int which) {
 #if LBM_BATCH_ARGS_SMEM

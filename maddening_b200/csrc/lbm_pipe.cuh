@@ -1,0 +1,110 @@
+// D3Q7 passive tracer of the pipe node (MADDENING LBMPipeNode.update, tracer
+// branch, src/maddening/nodes/lbm_pipe.py:857-871):
+//   tracer = sum g;  g_eq_q = w7_q tracer (1 + e_q.u / cs2)   (u: this step's
+//   new velocity, 0 in walls);  g_post = g in walls, else g - (g - g_eq)/tau_t;
+//   g_str = periodic shift by e_q;  g_bc = where(wall, g_str[opp], g_str);
+//   tracer_out = sum g_bc (0 in walls).
+// The collision needs the velocity of the same step at the same cell, which
+// the D3Q19 pass writes first, so the tracer runs as its own pass in push
+// form: a cell collides its own populations and sends population q to
+// y = x + e_q, into slot opp(q) when y is a wall (the wall swap taken at the
+// destination; every slot is written exactly once).  Populations are FP32
+// (FP64 with FP64 plans), one plane per direction.
+#pragma once
+
+#include "lbm_kernels.cuh"
+
+namespace lbm {
+
+struct Lat7 {
+  __host__ __device__ static constexpr int c(int q, int a) {
+    // rest, +x, -x, +y, -y, +z, -z (the first seven D3Q19 directions)
+    return q == 0 ? 0 : ((q - 1) / 2 == a ? ((q & 1) ? 1 : -1) : 0);
+  }
+  __host__ __device__ static constexpr int opp(int q) { return q == 0 ? 0 : ((q & 1) ? q + 1 : q - 1); }
+  __host__ __device__ static constexpr double w(int q) { return q == 0 ? 0.25 : 0.125; }
+};
+
+struct TracerArgs {
+  Geo g;
+  const uint8_t* wall;
+  const void* tin;      // populations (7 planes)
+  void* tout;
+  const void* vel;      // (grid, 3) velocity of this step, 0 in walls
+  double inv_tau;       // 1 / tau_tracer
+  const void* f7_in;    // (grid, 7) reference layout (prepare)
+  void* f7_out;         // (grid, 7) reference layout (final)
+  void* tracer_out;     // grid (final)
+};
+
+template <class IO>
+__global__ void __launch_bounds__(kBlock) k_tracer_prepare(const TracerArgs a) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= a.g.ncell) return;
+  const IO* fi = static_cast<const IO*>(a.f7_in) + static_cast<size_t>(c) * 7;
+#pragma unroll
+  for (int q = 0; q < 7; ++q) static_cast<IO*>(a.tout)[static_cast<size_t>(q) * a.g.ncell + c] = fi[q];
+}
+
+template <class IO>
+__global__ void __launch_bounds__(kBlock) k_tracer_step(const TracerArgs a) {
+  const Geo& g = a.g;
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= g.ncell) return;
+  const Cell x = locate(g, c);
+  const IO* tin = static_cast<const IO*>(a.tin);
+  IO t[7];
+#pragma unroll
+  for (int q = 0; q < 7; ++q) t[q] = tin[static_cast<size_t>(q) * g.ncell + c];
+  const bool wall = a.wall != nullptr && a.wall[c] != 0;
+  if (!wall) {
+    IO tracer = t[0];
+#pragma unroll
+    for (int q = 1; q < 7; ++q) tracer = add_r(tracer, t[q]);
+    const IO* u = static_cast<const IO*>(a.vel) + static_cast<size_t>(c) * 3;
+    const IO uu[3] = {u[0], u[1], u[2]};
+    const IO it = static_cast<IO>(a.inv_tau);
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      IO eu = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        if (Lat7::c(q, d)) eu = Lat7::c(q, d) > 0 ? uu[d] : -uu[d];
+      const IO geq = mul_r(mul_r(static_cast<IO>(Lat7::w(q)), tracer), fma_r(IO(3), eu, IO(1)));
+      t[q] = fma_r(-it, sub_r(t[q], geq), t[q]);
+    }
+  }
+  IO* tout = static_cast<IO*>(a.tout);
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    const uint32_t j0 = wrapu(static_cast<int>(x.i0) + Lat7::c(q, 0), g.n0);
+    const uint32_t j1 = wrapu(static_cast<int>(x.i1) + Lat7::c(q, 1), g.n1);
+    const uint32_t j2 = wrapu(static_cast<int>(x.k) + Lat7::c(q, 2), g.n2);
+    const uint32_t y = (j0 * g.n1 + j1) * g.n2 + j2;
+    const bool wy = a.wall != nullptr && a.wall[y] != 0;
+    const int slot = wy ? Lat7::opp(q) : q;
+    tout[static_cast<size_t>(slot) * g.ncell + y] = t[q];
+  }
+}
+
+// Last pass: populations to the reference layout and the tracer field.
+template <class IO>
+__global__ void __launch_bounds__(kBlock) k_tracer_final(const TracerArgs a) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= a.g.ncell) return;
+  const IO* tin = static_cast<const IO*>(a.tin);
+  IO* fo = static_cast<IO*>(a.f7_out) + static_cast<size_t>(c) * 7;
+  IO s = 0;
+#pragma unroll
+  for (int q = 0; q < 7; ++q) {
+    const IO v = tin[static_cast<size_t>(q) * a.g.ncell + c];
+    fo[q] = v;
+    s = q == 0 ? v : add_r(s, v);
+  }
+  if (a.tracer_out != nullptr) {
+    const bool wall = a.wall != nullptr && a.wall[c] != 0;
+    static_cast<IO*>(a.tracer_out)[c] = wall ? IO(0) : s;
+  }
+}
+
+}  // namespace lbm

@@ -126,6 +126,14 @@ def _make_jnp():
     jnp.where = lambda c, a, b: _wrap(np.where(_plain(c), _plain(a), _plain(b)))
     jnp.broadcast_to = lambda x, shape: _wrap(np.broadcast_to(_plain(x), shape))
     jnp.pad = lambda x, w: _wrap(np.pad(_plain(x), w))
+    jnp.arange = lambda *a, dtype=None: _wrap(np.arange(*a, dtype=dtype))
+    jnp.meshgrid = lambda *xs, indexing="xy": tuple(
+        _wrap(np.array(m)) for m in np.meshgrid(*[_plain(x) for x in xs], indexing=indexing))
+    jnp.sqrt = lambda x: _wrap(np.sqrt(_plain(x)))
+    jnp.exp = lambda x: _wrap(np.exp(_plain(x)))
+    jnp.tanh = lambda x: _wrap(np.tanh(_plain(x)))
+    jnp.clip = lambda x, lo, hi: _wrap(np.clip(_plain(x), lo, hi))
+    jnp.minimum = lambda a, b: _wrap(np.minimum(_plain(a), _plain(b)))
     jnp.all = lambda x: bool(np.all(_plain(x)))
     jnp.isfinite = lambda x: _wrap(np.isfinite(_plain(x)))
     jnp.ndarray = JArray
@@ -375,6 +383,39 @@ def run_padded_case(lbm, jnp, case, mode, seed):
     return out
 
 
+PIPE_CASES = [
+    # LBMPipeNode (lbm_pipe.py:393-879), single phase
+    dict(name="pipe_propeller_gravity_partial_fill", nx=12, ny=10, nz=10, tau=0.8,
+         pipe_radius=0.9, propeller_x=3, propeller_radius=0.8, propeller_strength=5e-4,
+         initial_velocity=0.01, gravity=2e-5, fill_fraction=0.6, tau_tracer=0.6, steps=4,
+         bi={}),
+    dict(name="pipe_odd_dims_force_override", nx=9, ny=11, nz=8, tau=0.7,
+         pipe_radius=0.85, propeller_x=5, propeller_radius=0.7, propeller_strength=3e-4,
+         initial_velocity=0.0, gravity=0.0, fill_fraction=1.0, tau_tracer=0.75, steps=3,
+         bi={"propeller_force": 8e-4}),
+]
+
+
+def run_pipe_case(pipe, jnp, case, mode):
+    kw = {k: v for k, v in case.items() if k not in ("name", "steps", "bi")}
+    node = pipe.LBMPipeNode(case["name"], 1.0, **kw)
+    st = node.initial_state()
+    out = {k + "0": np.asarray(_plain(v)) for k, v in st.items()}
+    if mode == "x64":
+        st = {k: jnp.asarray(np.asarray(_plain(v), dtype=np.float64)) for k, v in st.items()}
+    bi = {k: v for k, v in case["bi"].items()}
+    for step in range(case["steps"]):
+        st = node.update(st, bi, 1.0)
+        if step == 0:
+            for key in ("f", "density", "velocity", "tracer", "tracer_f"):
+                out["step1_" + key] = np.asarray(_plain(st[key]))
+    for key in ("f", "density", "velocity", "tracer", "tracer_f"):
+        out["final_" + key] = np.asarray(_plain(st[key]))
+    out["wall"] = np.asarray(_plain(node._wall_mask))
+    out["propeller"] = np.asarray(_plain(node._propeller_mask))
+    return out
+
+
 def unit_vectors(lbm, jnp, seed=7):
     """Golden vectors for the pure kernels on random inputs (x64)."""
     rng = np.random.default_rng(seed)
@@ -432,10 +473,17 @@ def main(ref_root="/root/reference"):
             res = run_padded_case(lbm, jnp, case, mode, seed=100 + i)
             for k, v in res.items():
                 golden[f"{case['name']}|{mode}|{k}"] = v
+    pipe = importlib.import_module("maddening.nodes.lbm_pipe")
+    for case in PIPE_CASES:
+        for mode in ("x64", "f32"):
+            MODE["value"] = mode
+            res = run_pipe_case(pipe, jnp, case, mode)
+            for k, v in res.items():
+                golden[f"{case['name']}|{mode}|{k}"] = v
     MODE["value"] = "x64"
     out = Path(__file__).with_name("lbm_golden.npz")
     np.savez_compressed(out, **golden)
-    meta = {c["name"]: c for c in CASES + PADDED_CASES}
+    meta = {c["name"]: c for c in CASES + PADDED_CASES + PIPE_CASES}
     print(f"wrote {out} ({out.stat().st_size / 1024:.1f} KiB, {len(golden)} arrays, "
           f"{len(meta)} cases)")
 
