@@ -313,6 +313,8 @@ def run_ours(args):
         variants["adjoint"] = adjoint_cost(dev)
         torch.cuda.empty_cache()
         variants["batched"] = batched_cost(dev)
+        torch.cuda.empty_cache()
+        variants["pipe"] = pipe_cost(dev)
 
     if rank == 0:
         peak, peak_kind = _peaks()
@@ -456,6 +458,46 @@ def batched_cost(dev, steps=500):
     out["batched_f16_over_plain_f32"] = round(out["batched_f16_mlups"] / ref, 3)
     out["hbm_frac_batched_f32"] = round(out["batched_f32_mlups"] * 1e6 * 152 / 1e9 / _peaks()[0], 4)
     out["hbm_frac_batched_f16"] = round(out["batched_f16_mlups"] * 1e6 * 76 / 1e9 / _peaks()[0], 4)
+    return out
+
+
+def pipe_cost(dev, steps=200):
+    """The pipe node (LBMPipeNode) on a 384 x 192 x 192 pipe (14.2 M cells,
+    radius 0.9, propeller disc at x = 96), FP32, best of three K-step runs of
+    ``run`` (populations in and out in the reference layout):
+    single phase (propeller 4e-4, gravity -1e-5, 70% fill) and Shan-Chen
+    multiphase (G = -4.5, liquid 1.3 / gas 0.3, half filled).  Bytes per cell
+    and step of the passes as built: single phase 152 (D3Q19 step) + 12
+    (velocity for the tracer) + 12 + 56 (D3Q7 tracer step) = 232; multiphase
+    76 + 4 (density pass) + 76 + 4 + 76 (collide and push) = 236."""
+    import torch
+    from maddening_b200.pipe import LBMPipeNode
+    out = {"workload": "384x192x192 pipe, FP32, %d steps" % steps}
+    kw = dict(nx=384, ny=192, nz=192, tau=0.8, pipe_radius=0.9, propeller_x=96,
+              propeller_radius=0.8, propeller_strength=4e-4, initial_velocity=0.005,
+              gravity=-1e-5, tau_tracer=0.6)
+    modes = {"single_phase": (dict(fill_fraction=0.7), 232),
+             "multiphase": (dict(fill_fraction=0.5, G=-4.5, rho_liquid=1.3, rho_gas=0.3), 236)}
+    for name, (extra, bpc) in modes.items():
+        node = LBMPipeNode("bench_pipe", 1.0, device=dev, **kw, **extra)
+        st = node.initial_state()
+        node.run(st, {}, 3)
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            node.run(st, {}, steps)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        cells = 384 * 192 * 192
+        m = cells * steps / best / 1e6
+        out[name] = {"mlups": round(m, 1), "bytes_per_cell": bpc,
+                     "hbm_frac": round(m * 1e6 * bpc / 1e9 / _peaks()[0], 4)}
+        del node, st
+        torch.cuda.empty_cache()
     return out
 
 

@@ -199,13 +199,19 @@ int lbm_rollout_history(const lbm_plan* plan, lbm_stream_t stream, const void* f
                         const lbm_history* history, void* workspace, size_t workspace_bytes);
 
 /* ---- Pipe node -----------------------------------------------------------
- * MADDENING's LBMPipeNode (src/maddening/nodes/lbm_pipe.py:393-879), single
- * phase: D3Q19 BGK with the Guo source of an actuator-disc propeller (x force
- * on the disc cells of plane propeller_x) and gravity (z force on every
- * non-wall cell), moments without the half-force step, periodic stream,
- * wall-node swap; then the D3Q7 passive tracer collided with the step's new
- * velocity (not in walls), streamed and wall-swapped.  The plan is D3Q19 with
- * FP32 or FP64 storage. */
+ * MADDENING's LBMPipeNode (src/maddening/nodes/lbm_pipe.py:393-879).
+ * Single phase (G == 0): D3Q19 BGK with the Guo source of an actuator-disc
+ * propeller (x force on the disc cells of plane propeller_x) and gravity (z
+ * force on every non-wall cell), moments without the half-force step,
+ * periodic stream, wall-node swap; then the D3Q7 passive tracer collided with
+ * the step's new velocity (not in walls), streamed and wall-swapped.
+ * Multiphase (G != 0, lbm_pipe.py:775-864): the Shan-Chen force of the
+ * Yuan-Schaefer pseudopotential psi = rho_0 (1 - exp(-rho / rho_0)) (walls at
+ * psi(rho_wall), force 0 in walls) added to the propeller and gravity, exact-
+ * difference forcing with the shifted velocity clamped to |u| <= 0.25, the
+ * density floor 0.01 after the stream, tracer = clip((rho - rho_gas) /
+ * (rho_liquid - rho_gas), 0, 1); tracer_f is copied through unchanged.
+ * The plan is D3Q19 with FP32 or FP64 storage. */
 typedef struct {
   const uint8_t* wall;       /* grid, nonzero = wall                                */
   const uint8_t* propeller;  /* (ny, nz) disc mask of the propeller plane, or NULL */
@@ -213,6 +219,10 @@ typedef struct {
   double propeller_force;    /* x force on the disc cells                          */
   double gravity;            /* z force on the non-wall cells                      */
   double tau_tracer;         /* tracer relaxation time, > 0.5                      */
+  double G;                  /* Shan-Chen interaction strength; 0 = single phase   */
+  double rho_liquid, rho_gas;/* multiphase: rho_liquid > rho_gas > 0               */
+  double rho_0;              /* multiphase: pseudopotential density, > 0           */
+  double rho_wall;           /* multiphase: density that sets psi in wall cells    */
 } lbm_pipe_args;
 
 int lbm_pipe_workspace_bytes(const lbm_plan* plan, size_t* bytes);

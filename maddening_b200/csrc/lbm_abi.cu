@@ -15,6 +15,7 @@
 #include "lbm_adjoint.cuh"
 #include "lbm_kernels.cuh"
 #include "lbm_pair.cuh"
+#include "lbm_multiphase.cuh"
 #include "lbm_pipe.cuh"
 #include "lbm_staged.cuh"
 
@@ -1048,6 +1049,58 @@ int run_pipe(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_i
   return cuda_check(cudaGetLastError(), "k_tracer_final launch");
 }
 
+// Multiphase pipe step (G != 0): two passes per step over pre-collision
+// population planes (lbm_multiphase.cuh); the workspace holds two population
+// sets and the psi plane, inside the single-phase layout.
+template <class R>
+int run_pipe_mp(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a,
+                const lbm_pipe_args* pa, const void* f_in, void* f_out, const void* t_in,
+                void* t_out, int64_t n, const lbm_moments* out, void* tracer_out, char* ws) {
+  const size_t cells = p->g.ncell;
+  const size_t sb = align256(state_bytes(p));
+  char* A = ws;
+  char* B = ws + sb;
+  lbm::MPArgs m{};
+  m.s = a;
+  m.G = pa->G;
+  m.rho0 = pa->rho_0;
+  m.psi_wall = pa->rho_0 * (1.0 - std::exp(-pa->rho_wall / pa->rho_0));
+  m.rho_gas = pa->rho_gas;
+  m.drho = pa->rho_liquid - pa->rho_gas;
+  m.psi = ws + 2 * sb;
+  m.f_aos_in = f_in;
+  m.fin = A;
+  const unsigned grid = grid_for(p->g.ncell);
+  lbm::k_mp_density<R, lbm::kMPFirst><<<grid, lbm::kBlock, 0, s>>>(m);
+  int rc = cuda_check(cudaGetLastError(), "k_mp_density launch");
+  if (rc) return rc;
+  for (int64_t i = 0; i < n; ++i) {
+    m.fin = A;
+    m.fout = B;
+    lbm::k_mp_collide<R><<<grid, lbm::kBlock, 0, s>>>(m);
+    rc = cuda_check(cudaGetLastError(), "k_mp_collide launch");
+    if (rc) return rc;
+    std::swap(A, B);
+    if (i + 1 < n) {
+      m.fin = A;
+      lbm::k_mp_density<R, lbm::kMPStep><<<grid, lbm::kBlock, 0, s>>>(m);
+      rc = cuda_check(cudaGetLastError(), "k_mp_density launch");
+      if (rc) return rc;
+    }
+  }
+  m.fin = A;
+  m.f_aos_out = f_out;
+  m.rho_out = out != nullptr ? out->density : nullptr;
+  m.vel_out = out != nullptr ? out->velocity : nullptr;
+  m.tracer_out = tracer_out;
+  lbm::k_mp_density<R, lbm::kMPLast><<<grid, lbm::kBlock, 0, s>>>(m);
+  rc = cuda_check(cudaGetLastError(), "k_mp_density launch");
+  if (rc) return rc;
+  // tracer_f is not evolved in multiphase mode (lbm_pipe.py:858-860)
+  return cuda_check(cudaMemcpyAsync(t_out, t_in, 7 * cells * sizeof(R), cudaMemcpyDeviceToDevice, s),
+                    "tracer_f copy");
+}
+
 }  // namespace
 
 extern "C" {
@@ -1070,6 +1123,13 @@ int lbm_pipe_rollout(const lbm_plan* p, lbm_stream_t stream, const void* f_in, v
     return fail(LBM_ERR_INVALID, "f / tracer_f is NULL");
   if (n_steps < 1) return fail(LBM_ERR_INVALID, "n_steps must be >= 1 (got %lld)", (long long)n_steps);
   if (!(pa->tau_tracer > 0.5)) return fail(LBM_ERR_INVALID, "tau_tracer must be > 0.5");
+  if (pa->G != 0.0) {
+    if (!(pa->rho_liquid > pa->rho_gas))
+      return fail(LBM_ERR_INVALID, "rho_liquid must be > rho_gas (got %g <= %g)", pa->rho_liquid,
+                  pa->rho_gas);
+    if (!(pa->rho_gas > 0.0)) return fail(LBM_ERR_INVALID, "rho_gas must be > 0");
+    if (!(pa->rho_0 > 0.0)) return fail(LBM_ERR_INVALID, "rho_0 must be > 0");
+  }
   if (pa->propeller != nullptr &&
       (pa->propeller_x < 0 || pa->propeller_x >= static_cast<int32_t>(p->g.n0)))
     return fail(LBM_ERR_INVALID, "propeller_x %d outside [0, %u)", pa->propeller_x, p->g.n0);
@@ -1091,6 +1151,13 @@ int lbm_pipe_rollout(const lbm_plan* p, lbm_stream_t stream, const void* f_in, v
   a.prop_mask = pa->propeller;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   char* ws = static_cast<char*>(workspace);
+  if (pa->G != 0.0) {
+    if (p->storage == LBM_STORE_F32)
+      return run_pipe_mp<float>(p, s, a, pa, f_in, f_out, tracer_f_in, tracer_f_out, n_steps, out,
+                                tracer_out, ws);
+    return run_pipe_mp<double>(p, s, a, pa, f_in, f_out, tracer_f_in, tracer_f_out, n_steps, out,
+                               tracer_out, ws);
+  }
   if (p->storage == LBM_STORE_F32)
     return run_pipe<float>(p, s, a, f_in, f_out, tracer_f_in, tracer_f_out, n_steps,
                            pa->tau_tracer, tracer_out, ws);

@@ -1,0 +1,230 @@
+// Shan-Chen multiphase step of the pipe node (MADDENING LBMPipeNode.update
+// with G != 0, src/maddening/nodes/lbm_pipe.py:751-864; the interaction force
+// is _shan_chen_force, lbm_pipe.py:321-375):
+//   rho, u   = moments(f) (no half-force step), u = m / max(rho, 1e-10)
+//   psi(y)   = psi_wall in walls, else rho_0 (1 - exp(-rho(y) / rho_0))
+//   F        = propeller + gravity + (0 in walls) -G psi(x) sum_q w_q psi(x + e_q) e_q
+//   u_s      = u + F / max(rho, 0.01), scaled down to |u_s| <= 0.25
+//   f*       = f - (f - feq(rho, u)) / tau + (feq(rho, u_s) - feq(rho, u))   (exact difference)
+//   f_bc     = periodic stream of f*, wall-node swap
+//   floor    : where sum f_bc < 0.01, f_bc *= 0.01 / sum f_bc and rho = 0.01
+//   outputs  : rho, u = moments(f_bc) (0 in walls), tracer = clip((rho - rho_gas) /
+//              (rho_liquid - rho_gas), 0, 1) (0 in walls); tracer_f passes through.
+//
+// The force at x needs psi at the 18 neighbours, i.e. the density of every
+// cell before any cell collides, so a step is two passes over populations
+// kept PRE-collision in FP32 (FP64 for FP64 plans) planes, one per direction:
+//   k_mp_density  reads f, applies the floor (rewriting the rare floored cell),
+//                 writes psi (one plane);
+//   k_mp_collide  reads f and psi of the neighbours, collides, and pushes
+//                 population q to y = x + e_q, into slot opp(q) when y is a
+//                 wall (the wall swap taken at the destination; every slot is
+//                 written exactly once).
+// Traffic per cell and step: 19 loads + 1 psi store, then 19 loads + 19
+// stores + the psi loads (mostly cache hits).
+#pragma once
+
+#include "lbm_kernels.cuh"
+
+namespace lbm {
+
+struct MPArgs {
+  StepArgs s;            // geometry, wall, omega, pipe force (force_mode 3 fields)
+  double G, rho0;        // interaction strength, pseudopotential density
+  double psi_wall;       // rho_0 (1 - exp(-rho_wall / rho_0))
+  double rho_gas, drho;  // tracer = (rho - rho_gas) / drho, drho = rho_liquid - rho_gas
+  const void* fin;       // population planes
+  void* fout;
+  void* psi;             // psi plane
+  const void* f_aos_in;  // (grid, 19) reference layout (first pass)
+  void* f_aos_out;       // (grid, 19) reference layout (last pass)
+  void* rho_out;         // grid (last pass)
+  void* vel_out;         // (grid, 3) (last pass)
+  void* tracer_out;      // grid (last pass; NULL = not written)
+};
+
+constexpr int kMPFirst = 0;  // f from the reference layout, no floor, psi
+constexpr int kMPStep = 1;   // floor in place, psi
+constexpr int kMPLast = 2;   // floor, f to the reference layout, outputs
+
+template <class R>
+__device__ __forceinline__ R sum19(const R (&f)[19]) {
+  R s = f[0];
+#pragma unroll
+  for (int q = 1; q < 19; ++q) s = add_r(s, f[q]);
+  return s;
+}
+
+template <class R>
+__device__ __forceinline__ void mom19(const R (&f)[19], R (&m)[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    R acc = 0;
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+      const int e = d == 0 ? Lat<19>::c0(q) : (d == 1 ? Lat<19>::c1(q) : Lat<19>::c2(q));
+      if (e > 0) acc = add_r(acc, f[q]);
+      if (e < 0) acc = sub_r(acc, f[q]);
+    }
+    m[d] = acc;
+  }
+}
+
+__device__ __forceinline__ float sqrt_r(float x) { return __fsqrt_rn(x); }
+__device__ __forceinline__ double sqrt_r(double x) { return __dsqrt_rn(x); }
+__device__ __forceinline__ float expm1_r(float x) { return expm1f(x); }
+__device__ __forceinline__ double expm1_r(double x) { return expm1(x); }
+
+// psi(rho) = rho_0 (1 - exp(-rho / rho_0)), lbm_pipe.py:301-318, written with
+// expm1 so that small densities keep their relative precision.
+template <class R>
+__device__ __forceinline__ R psi_of(R rho, R rho0) {
+  return mul_r(rho0, -expm1_r(div_r(-rho, rho0)));
+}
+
+template <class R, int MODE>
+__global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
+  const Geo& g = a.s.g;
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= g.ncell) return;
+  R f[19];
+  if (MODE == kMPFirst) {
+    const R* fi = static_cast<const R*>(a.f_aos_in) + static_cast<size_t>(c) * 19;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = fi[q];
+  } else {
+    const R* fi = static_cast<const R*>(a.fin);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = fi[static_cast<size_t>(q) * g.ncell + c];
+  }
+  const bool wall = a.s.wall != nullptr && a.s.wall[c] != 0;
+  const R s0 = sum19(f);  // the new density before the floor
+  R m[3];
+  if (MODE == kMPLast) mom19(f, m);  // the output velocity is taken before the floor
+  R s = s0, rho_out = s0;
+  const R floor = static_cast<R>(0.01);
+  if (MODE != kMPFirst && s0 < floor) {  // lbm_pipe.py:838-848
+    const R ratio = div_r(floor, s0 > R(1e-20) ? s0 : R(1e-20));
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = mul_r(f[q], ratio);
+    if (MODE == kMPStep) {
+      R* fo = static_cast<R*>(const_cast<void*>(a.fin));
+#pragma unroll
+      for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + c] = f[q];
+    }
+    rho_out = floor;
+    s = sum19(f);  // what the next step sums for this cell
+  }
+  if (MODE == kMPFirst) {
+    R* fo = static_cast<R*>(const_cast<void*>(a.fin));
+#pragma unroll
+    for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + c] = f[q];
+  }
+  if (MODE != kMPLast) {
+    static_cast<R*>(a.psi)[c] =
+        wall ? static_cast<R>(a.psi_wall) : psi_of(s, static_cast<R>(a.rho0));
+    return;
+  }
+  R* fo = static_cast<R*>(a.f_aos_out) + static_cast<size_t>(c) * 19;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) fo[q] = f[q];
+  if (a.rho_out != nullptr) static_cast<R*>(a.rho_out)[c] = rho_out;
+  if (a.vel_out != nullptr) {
+    const R den = s0 > R(1e-10) ? s0 : R(1e-10);
+    R* v = static_cast<R*>(a.vel_out) + static_cast<size_t>(c) * 3;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = wall ? R(0) : div_r(m[d], den);
+  }
+  if (a.tracer_out != nullptr) {
+    R t = div_r(sub_r(rho_out, static_cast<R>(a.rho_gas)), static_cast<R>(a.drho));
+    t = t < R(0) ? R(0) : (t > R(1) ? R(1) : t);
+    static_cast<R*>(a.tracer_out)[c] = wall ? R(0) : t;
+  }
+}
+
+// Collide with the Shan-Chen force and exact-difference forcing, then push.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
+  const Geo& g = a.s.g;
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= g.ncell) return;
+  const Cell x = locate(g, c);
+  const R* fi = static_cast<const R*>(a.fin);
+  R f[19];
+#pragma unroll
+  for (int q = 0; q < 19; ++q) f[q] = fi[static_cast<size_t>(q) * g.ncell + c];
+  const uint8_t* wm = a.s.wall;
+  const bool wall = wm != nullptr && wm[c] != 0;
+  const R rho = sum19(f);
+  R m[3];
+  mom19(f, m);
+  const R den = rho > R(1e-10) ? rho : R(1e-10);
+  R u[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) u[d] = div_r(m[d], den);
+  R F[3];
+  pipe_force<R>(a.s, c, wall, F);
+  if (!wall) {
+    // sum_q w_q psi(x + e_q) e_q = (2 S_axis + S_diag) / 36
+    const R* psi = static_cast<const R*>(a.psi);
+    R s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0};
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+      const int e0 = Lat<19>::c0(q), e1 = Lat<19>::c1(q), e2 = Lat<19>::c2(q);
+      const uint32_t j0 = wrapu(static_cast<int>(x.i0) + e0, g.n0);
+      const uint32_t j1 = wrapu(static_cast<int>(x.i1) + e1, g.n1);
+      const uint32_t j2 = wrapu(static_cast<int>(x.k) + e2, g.n2);
+      const R p = __ldg(psi + (j0 * g.n1 + j1) * g.n2 + j2);
+      R(&acc)[3] = q <= 6 ? s1 : s2;
+      if (e0) acc[0] = e0 > 0 ? add_r(acc[0], p) : sub_r(acc[0], p);
+      if (e1) acc[1] = e1 > 0 ? add_r(acc[1], p) : sub_r(acc[1], p);
+      if (e2) acc[2] = e2 > 0 ? add_r(acc[2], p) : sub_r(acc[2], p);
+    }
+    const R coef = mul_r(static_cast<R>(-a.G), __ldg(psi + c));
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      F[d] = fma_r(coef, div_r(fma_r(R(2), s1[d], s2[d]), R(36)), F[d]);
+  }
+  // shifted velocity u + F / max(rho, 0.01), clamped to |u_s| <= 0.25
+  const R rs = rho > R(0.01) ? rho : static_cast<R>(0.01);
+  R us[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) us[d] = add_r(u[d], div_r(F[d], rs));
+  const R umag = sqrt_r(fma_r(us[0], us[0], fma_r(us[1], us[1], mul_r(us[2], us[2]))));
+  const R umax = umag > R(1e-10) ? umag : R(1e-10);
+  const R scale = div_r(R(0.25), umax);
+  if (scale < R(1)) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) us[d] = mul_r(us[d], scale);
+  }
+  const R omega = static_cast<R>(a.s.omega);
+  const R usq_b = fma_r(u[0], u[0], fma_r(u[1], u[1], mul_r(u[2], u[2])));
+  const R usq_s = fma_r(us[0], us[0], fma_r(us[1], us[1], mul_r(us[2], us[2])));
+  const R dusq = sub_r(usq_s, usq_b);
+  const R r36 = div_r(rho, R(36));
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const R wr = mul_r(static_cast<R>(Lat<19>::wr(q)), r36);  // w_q rho
+    const R eb = dot_e(Lat<19>::c0(q), Lat<19>::c1(q), Lat<19>::c2(q), u);
+    const R es = dot_e(Lat<19>::c0(q), Lat<19>::c1(q), Lat<19>::c2(q), us);
+    // feq(rho, u) = w rho (1 + 3 e.u + 4.5 (e.u)^2 - 1.5 u.u)
+    const R feq = mul_r(wr, fma_r(eb, fma_r(R(4.5), eb, R(3)), fma_r(R(-1.5), usq_b, R(1))));
+    // feq(rho, u_s) - feq(rho, u) = w rho (3 de + 4.5 de (es + eb) - 1.5 d(u.u))
+    const R de = sub_r(es, eb);
+    const R dfeq =
+        mul_r(wr, fma_r(de, fma_r(R(4.5), add_r(es, eb), R(3)), mul_r(R(-1.5), dusq)));
+    f[q] = add_r(fma_r(-omega, sub_r(f[q], feq), f[q]), dfeq);
+  }
+  R* fo = static_cast<R*>(a.fout);
+#pragma unroll
+  for (int q = 0; q < 19; ++q) {
+    const uint32_t j0 = wrapu(static_cast<int>(x.i0) + Lat<19>::c0(q), g.n0);
+    const uint32_t j1 = wrapu(static_cast<int>(x.i1) + Lat<19>::c1(q), g.n1);
+    const uint32_t j2 = wrapu(static_cast<int>(x.k) + Lat<19>::c2(q), g.n2);
+    const uint32_t y = (j0 * g.n1 + j1) * g.n2 + j2;
+    const int slot = (wm != nullptr && __ldg(wm + y) != 0) ? Lat<19>::opp(q) : q;
+    fo[static_cast<size_t>(slot) * g.ncell + y] = f[q];
+  }
+}
+
+}  // namespace lbm

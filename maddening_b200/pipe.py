@@ -1,17 +1,20 @@
 """``LBMPipeNode``: MADDENING's pipe-flow node on the B200 kernels.
 
-Drop-in for ``src/maddening/nodes/lbm_pipe.py:393-879`` in single-phase mode
-(``G == 0``): D3Q19 fluid in a cylindrical pipe along x, driven by an
-actuator-disc propeller (x body force on one cross-section) and optional
-gravity (-z is the reference's sign convention: the value is added to the z
-force of every fluid cell), periodic in x, bounce-back pipe walls, plus a D3Q7
-passive tracer advected by the flow.  Same constructor arguments, validation,
-masks, state keys (``f``, ``density``, ``velocity``, ``tracer``, ``tracer_f``)
-and boundary input (``propeller_force``).  The step runs in ``liblbm_b200.so``
-(``lbm_pipe_rollout``); there is no CPU path.
+Drop-in for ``src/maddening/nodes/lbm_pipe.py:393-879``: D3Q19 fluid in a
+cylindrical pipe along x, driven by an actuator-disc propeller (x body force
+on one cross-section) and optional gravity (the value is added to the z force
+of every fluid cell), periodic in x, bounce-back pipe walls.  Same constructor
+arguments, validation, masks, state keys (``f``, ``density``, ``velocity``,
+``tracer``, ``tracer_f``) and boundary input (``propeller_force``).
 
-Multiphase mode (``G != 0``: Shan-Chen pseudopotential with exact-difference
-forcing) is not provided by this node yet and raises ``NotImplementedError``.
+* ``G == 0`` (single phase): BGK with the Guo source, plus a D3Q7 passive
+  tracer advected by the flow.
+* ``G != 0`` (multiphase): Shan-Chen pseudopotential force with
+  exact-difference forcing, a density floor, and the tracer read off the
+  density (``tracer_f`` passes through).
+
+The step runs in ``liblbm_b200.so`` (``lbm_pipe_rollout``); there is no CPU
+path.
 """
 
 from __future__ import annotations
@@ -36,7 +39,8 @@ _CS2 = 1.0 / 3.0
 class lbm_pipe_args(C.Structure):
     _fields_ = [("wall", C.c_void_p), ("propeller", C.c_void_p), ("propeller_x", C.c_int32),
                 ("propeller_force", C.c_double), ("gravity", C.c_double),
-                ("tau_tracer", C.c_double)]
+                ("tau_tracer", C.c_double), ("G", C.c_double), ("rho_liquid", C.c_double),
+                ("rho_gas", C.c_double), ("rho_0", C.c_double), ("rho_wall", C.c_double)]
 
 
 def _lib_pipe():
@@ -122,9 +126,6 @@ class LBMPipeNode(SimulationNode):
                 raise ValueError(f"rho_gas must be > 0 (got {rho_gas}).")
             if rho_0 <= 0.0:
                 raise ValueError(f"rho_0 must be > 0 (got {rho_0}).")
-            raise NotImplementedError(
-                "LBMPipeNode (B200): the Shan-Chen multiphase mode (G != 0) is not provided; "
-                "single-phase (G = 0) only")
         if storage not in ("f32", "f64"):
             raise ValueError(f"storage must be 'f32' or 'f64' (got {storage!r})")
         if rho_wall is None:
@@ -139,6 +140,9 @@ class LBMPipeNode(SimulationNode):
         self._tau, self._tau_tracer = float(tau), float(tau_tracer)
         self._gravity = float(gravity)
         self._fill_fraction = float(fill_fraction)
+        self._G = float(G)
+        self._rho_liquid, self._rho_gas = float(rho_liquid), float(rho_gas)
+        self._rho_0, self._rho_wall = float(rho_0), float(rho_wall)
         self._storage = storage
         self._io_dtype = torch.float64 if storage == "f64" else torch.float32
         self._device = torch.device(device) if device is not None else None
@@ -206,19 +210,43 @@ class LBMPipeNode(SimulationNode):
         liquid = (zz <= z_cutoff) & interior & ~near
         return np.broadcast_to(liquid[None], (self._nx, ny, nz))
 
+    def _multiphase_density(self) -> np.ndarray:
+        """lbm_pipe.py:677-711: liquid below the fill level, gas above, joined
+        by a tanh profile 5 cells wide; rho_gas in the walls."""
+        ny, nz = self._ny, self._nz
+        y = np.arange(ny, dtype=np.float32)
+        z = np.arange(nz, dtype=np.float32)
+        _, zz = np.meshgrid(y, z, indexing="ij")
+        interior = ~self._wall_np[0]
+        if self._fill_fraction >= 1.0:
+            z_cutoff = float(nz)
+        else:
+            z_cutoff = float(np.percentile(zz[interior], self._fill_fraction * 100))
+        phase = 0.5 * (1.0 + np.tanh((z_cutoff - np.arange(nz, dtype=np.float32)) / 5.0))
+        phase_3d = np.broadcast_to(phase[None, None, :], (self._nx, ny, nz))
+        density = self._rho_gas + (self._rho_liquid - self._rho_gas) * phase_3d
+        return np.where(self._wall_np, self._rho_gas, density).astype(np.float32)
+
     def initial_state(self) -> dict:
-        """lbm_pipe.py:664-749 (single phase): uniform x velocity in the pipe,
-        rho = 1, f = f_eq, tracer = 1 in the (filled part of the) pipe."""
+        """lbm_pipe.py:664-749: uniform x velocity in the pipe, f = f_eq.
+        Single phase: rho = 1, tracer = 1 in the (filled part of the) pipe.
+        Multiphase: the tanh density profile, tracer read off the density."""
         dev = self._dev()
         fluid = ~self._wall_np
         shape = (self._nx, self._ny, self._nz)
         velocity = np.zeros(shape + (3,), dtype=np.float32)
         velocity[..., 0] = np.where(fluid, np.float32(self.params["initial_velocity"]),
                                     np.float32(0.0))
-        density = np.ones(shape, dtype=np.float32)
+        if self._G != 0.0:
+            density = self._multiphase_density()
+            tracer = np.clip((density - self._rho_gas) / (self._rho_liquid - self._rho_gas),
+                             0.0, 1.0)
+            tracer = np.where(self._wall_np, 0.0, tracer).astype(np.float32)
+        else:
+            density = np.ones(shape, dtype=np.float32)
+            liquid = fluid if self._fill_fraction >= 1.0 else self._fill_mask()
+            tracer = np.where(liquid, 1.0, 0.0).astype(np.float32)
         f = _equilibrium(density, velocity).astype(np.float32)
-        liquid = fluid if self._fill_fraction >= 1.0 else self._fill_mask()
-        tracer = np.where(liquid, 1.0, 0.0).astype(np.float32)
         tracer_f = _tracer_equilibrium(tracer, velocity).astype(np.float32)
         to = lambda a: torch.as_tensor(a, device=dev).to(self._io_dtype)  # noqa: E731
         return {"f": to(f), "density": to(density), "velocity": to(velocity),
@@ -251,6 +279,9 @@ class LBMPipeNode(SimulationNode):
         a.propeller_force = float(s)
         a.gravity = self._gravity
         a.tau_tracer = self._tau_tracer
+        a.G = self._G
+        a.rho_liquid, a.rho_gas = self._rho_liquid, self._rho_gas
+        a.rho_0, a.rho_wall = self._rho_0, self._rho_wall
         f_out = torch.empty_like(f)
         g_out = torch.empty_like(g)
         rho = torch.empty(shape, dtype=self._io_dtype, device=dev)
@@ -270,7 +301,7 @@ class LBMPipeNode(SimulationNode):
                 "tracer_f": g_out}
 
     def update(self, state: dict, boundary_inputs: dict, dt: float) -> dict:
-        """One step of lbm_pipe.py:751-879 (single phase)."""
+        """One step of lbm_pipe.py:751-879."""
         return self._advance(state, boundary_inputs, 1)
 
     def run(self, state: dict, boundary_inputs: dict, n_steps: int) -> dict:

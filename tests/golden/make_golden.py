@@ -393,13 +393,35 @@ PIPE_CASES = [
          pipe_radius=0.85, propeller_x=5, propeller_radius=0.7, propeller_strength=3e-4,
          initial_velocity=0.0, gravity=0.0, fill_fraction=1.0, tau_tracer=0.75, steps=3,
          bi={"propeller_force": 8e-4}),
+    # multiphase (Shan-Chen pseudopotential with exact-difference forcing)
+    dict(name="pipe_multiphase_partial_fill", nx=10, ny=10, nz=12, tau=0.9,
+         pipe_radius=0.9, propeller_x=4, propeller_radius=0.8, propeller_strength=5e-4,
+         initial_velocity=0.01, gravity=-1e-5, fill_fraction=0.5, tau_tracer=0.6, G=-4.5,
+         rho_liquid=1.3, rho_gas=0.3, rho_0=1.0, steps=5, bi={}),
+    dict(name="pipe_multiphase_odd_dims_rho_wall", nx=8, ny=9, nz=11, tau=0.75,
+         pipe_radius=0.85, propeller_x=2, propeller_radius=0.7, propeller_strength=3e-4,
+         initial_velocity=0.0, gravity=0.0, fill_fraction=1.0, tau_tracer=0.6, G=-4.2,
+         rho_liquid=1.0, rho_gas=0.25, rho_0=1.0, rho_wall=0.5, steps=4,
+         bi={"propeller_force": 8e-4}),
+    # a near-empty block inside the liquid: the density floor rescales the
+    # populations and the shifted velocity is clamped at its rim
+    dict(name="pipe_multiphase_floor_and_clamp", nx=10, ny=10, nz=12, tau=0.8,
+         pipe_radius=0.9, propeller_x=2, propeller_radius=0.8, propeller_strength=5e-4,
+         initial_velocity=0.0, gravity=0.0, fill_fraction=1.0, tau_tracer=0.6, G=-6.0,
+         rho_liquid=2.5, rho_gas=0.2, rho_0=1.0, steps=3, bi={},
+         scale_block=((4, 7), (4, 7), (4, 7), 0.002)),
 ]
 
 
 def run_pipe_case(pipe, jnp, case, mode):
-    kw = {k: v for k, v in case.items() if k not in ("name", "steps", "bi")}
+    kw = {k: v for k, v in case.items() if k not in ("name", "steps", "bi", "scale_block")}
     node = pipe.LBMPipeNode(case["name"], 1.0, **kw)
     st = node.initial_state()
+    if "scale_block" in case:
+        (a0, a1), (b0, b1), (c0, c1), factor = case["scale_block"]
+        f = np.array(np.asarray(_plain(st["f"])), dtype=np.float32)
+        f[a0:a1, b0:b1, c0:c1] *= np.float32(factor)
+        st = dict(st, f=jnp.asarray(f))
     out = {k + "0": np.asarray(_plain(v)) for k, v in st.items()}
     if mode == "x64":
         st = {k: jnp.asarray(np.asarray(_plain(v), dtype=np.float64)) for k, v in st.items()}

@@ -1,6 +1,7 @@
 """LBMPipeNode host side (no GPU): the reference's validation, masks and
-contract surface (src/maddening/nodes/lbm_pipe.py:493-662), masks checked
-against the reference-executed golden fixtures."""
+contract surface (src/maddening/nodes/lbm_pipe.py:493-662), masks and the
+multiphase initial density checked against the reference-executed golden
+fixtures."""
 
 import numpy as np
 import pytest
@@ -10,7 +11,7 @@ from tests.golden.make_golden import PIPE_CASES
 
 
 def _kw(case):
-    return {k: v for k, v in case.items() if k not in ("name", "steps", "bi")}
+    return {k: v for k, v in case.items() if k not in ("name", "steps", "bi", "scale_block")}
 
 
 @pytest.mark.parametrize("case", PIPE_CASES, ids=[c["name"] for c in PIPE_CASES])
@@ -32,9 +33,22 @@ def test_validation_like_reference(kw, msg):
         LBMPipeNode("p", 1.0, nx=8, ny=8, nz=8, **kw)
 
 
-def test_multiphase_not_provided():
-    with pytest.raises(NotImplementedError, match="multiphase"):
-        LBMPipeNode("p", 1.0, nx=8, ny=8, nz=8, G=-4.5)
+MP_CASES = [c for c in PIPE_CASES if c.get("G", 0.0) != 0.0]
+
+
+@pytest.mark.parametrize("case", MP_CASES, ids=[c["name"] for c in MP_CASES])
+def test_multiphase_initial_density_matches_reference(golden, case):
+    node = LBMPipeNode(case["name"], 1.0, **_kw(case))
+    np.testing.assert_array_equal(node._multiphase_density(),
+                                  golden[f"{case['name']}|x64|density0"])
+
+
+def test_multiphase_parameters():
+    node = LBMPipeNode("p", 1.0, nx=8, ny=8, nz=8, G=-4.5, rho_liquid=1.2, rho_gas=0.3)
+    assert node.params["G"] == -4.5
+    assert node.params["rho_wall"] == 1.2
+    node = LBMPipeNode("p", 1.0, nx=8, ny=8, nz=8, G=-4.5, rho_wall=0.4)
+    assert node.params["rho_wall"] == 0.4
 
 
 def test_contract_surface():
