@@ -17,9 +17,13 @@
 //   k_mp_density  reads f, applies the floor (rewriting the rare floored cell),
 //                 writes psi (one plane);
 //   k_mp_collide  reads f and psi of the neighbours, collides, and pushes
-//                 population q to y = x + e_q, into slot opp(q) when y is a
-//                 wall (the wall swap taken at the destination; every slot is
-//                 written exactly once).
+//                 population q to y = x + e_q.
+// The planes hold the STREAMED populations f_str; the wall swap is deferred to
+// the readers: a wall cell's slots q and opp(q) are exchanged in registers when
+// the cell is loaded (the density is a permutation-invariant sum, and the
+// floor scales every slot alike), so the push needs no wall test at the
+// destination.  The first pass stores its input (the reference's f_bc) with
+// the same exchange, the last pass undoes it for the output.
 // Traffic per cell and step: 19 loads + 1 psi store, then 19 loads + 19
 // stores + the psi loads (mostly cache hits).
 #pragma once
@@ -70,6 +74,20 @@ __device__ __forceinline__ void mom19(const R (&f)[19], R (&m)[3]) {
   }
 }
 
+// Exchange slots q and opp(q): the wall-node swap of a wall cell.
+template <class R>
+__device__ __forceinline__ void swap_opp(R (&f)[19]) {
+#pragma unroll
+  for (int q = 1; q < 19; ++q) {
+    const int o = Lat<19>::opp(q);
+    if (q < o) {
+      const R t = f[q];
+      f[q] = f[o];
+      f[o] = t;
+    }
+  }
+}
+
 __device__ __forceinline__ float sqrt_r(float x) { return __fsqrt_rn(x); }
 __device__ __forceinline__ double sqrt_r(double x) { return __dsqrt_rn(x); }
 __device__ __forceinline__ float expm1_r(float x) { return expm1f(x); }
@@ -99,8 +117,11 @@ __global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
   }
   const bool wall = a.s.wall != nullptr && a.s.wall[c] != 0;
   const R s0 = sum19(f);  // the new density before the floor
-  R m[3];
-  if (MODE == kMPLast) mom19(f, m);  // the output velocity is taken before the floor
+  R m[3] = {0, 0, 0};
+  if (MODE == kMPLast) {
+    if (wall) swap_opp(f);  // to f_bc (no velocity is taken in walls)
+    else mom19(f, m);       // the output velocity is taken before the floor
+  }
   R s = s0, rho_out = s0;
   const R floor = static_cast<R>(0.01);
   if (MODE != kMPFirst && s0 < floor) {  // lbm_pipe.py:838-848
@@ -116,6 +137,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
     s = sum19(f);  // what the next step sums for this cell
   }
   if (MODE == kMPFirst) {
+    if (wall) swap_opp(f);  // f_bc -> the streamed form the planes hold
     R* fo = static_cast<R*>(const_cast<void*>(a.fin));
 #pragma unroll
     for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + c] = f[q];
@@ -155,13 +177,30 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   for (int q = 0; q < 19; ++q) f[q] = fi[static_cast<size_t>(q) * g.ncell + c];
   const uint8_t* wm = a.s.wall;
   const bool wall = wm != nullptr && wm[c] != 0;
-  const R rho = sum19(f);
+  const R rho = sum19(f);  // in the order of the density pass: the same value
+  if (wall) swap_opp(f);   // the deferred wall-node swap
+  // offsets of the periodic neighbours along each axis
+  const int32_t pl = static_cast<int32_t>(g.plane), rw = static_cast<int32_t>(g.n2);
+  const int32_t o0m = x.i0 == 0 ? (static_cast<int32_t>(g.n0) - 1) * pl : -pl;
+  const int32_t o0p = x.i0 + 1 == g.n0 ? -(static_cast<int32_t>(g.n0) - 1) * pl : pl;
+  const int32_t o1m = x.i1 == 0 ? (static_cast<int32_t>(g.n1) - 1) * rw : -rw;
+  const int32_t o1p = x.i1 + 1 == g.n1 ? -(static_cast<int32_t>(g.n1) - 1) * rw : rw;
+  const int32_t o2m = x.k == 0 ? rw - 1 : -1;
+  const int32_t o2p = x.k + 1 == g.n2 ? 1 - rw : 1;
+  auto nb = [&](int q) -> uint32_t {
+    const int e0 = Lat<19>::c0(q), e1 = Lat<19>::c1(q), e2 = Lat<19>::c2(q);
+    int32_t o = 0;
+    if (e0) o += e0 > 0 ? o0p : o0m;
+    if (e1) o += e1 > 0 ? o1p : o1m;
+    if (e2) o += e2 > 0 ? o2p : o2m;
+    return static_cast<uint32_t>(static_cast<int32_t>(c) + o);
+  };
   R m[3];
   mom19(f, m);
-  const R den = rho > R(1e-10) ? rho : R(1e-10);
+  const R inv_den = rcp_r(rho > R(1e-10) ? rho : R(1e-10));
   R u[3];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) u[d] = div_r(m[d], den);
+  for (int d = 0; d < 3; ++d) u[d] = mul_r(m[d], inv_den);
   R F[3];
   pipe_force<R>(a.s, c, wall, F);
   if (!wall) {
@@ -171,29 +210,25 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
 #pragma unroll
     for (int q = 1; q < 19; ++q) {
       const int e0 = Lat<19>::c0(q), e1 = Lat<19>::c1(q), e2 = Lat<19>::c2(q);
-      const uint32_t j0 = wrapu(static_cast<int>(x.i0) + e0, g.n0);
-      const uint32_t j1 = wrapu(static_cast<int>(x.i1) + e1, g.n1);
-      const uint32_t j2 = wrapu(static_cast<int>(x.k) + e2, g.n2);
-      const R p = __ldg(psi + (j0 * g.n1 + j1) * g.n2 + j2);
+      const R p = __ldg(psi + nb(q));
       R(&acc)[3] = q <= 6 ? s1 : s2;
       if (e0) acc[0] = e0 > 0 ? add_r(acc[0], p) : sub_r(acc[0], p);
       if (e1) acc[1] = e1 > 0 ? add_r(acc[1], p) : sub_r(acc[1], p);
       if (e2) acc[2] = e2 > 0 ? add_r(acc[2], p) : sub_r(acc[2], p);
     }
     const R coef = mul_r(static_cast<R>(-a.G), __ldg(psi + c));
+    const R inv36 = static_cast<R>(1.0 / 36.0);
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-      F[d] = fma_r(coef, div_r(fma_r(R(2), s1[d], s2[d]), R(36)), F[d]);
+    for (int d = 0; d < 3; ++d) F[d] = fma_r(coef, mul_r(fma_r(R(2), s1[d], s2[d]), inv36), F[d]);
   }
   // shifted velocity u + F / max(rho, 0.01), clamped to |u_s| <= 0.25
-  const R rs = rho > R(0.01) ? rho : static_cast<R>(0.01);
+  const R inv_rs = rcp_r(rho > R(0.01) ? rho : static_cast<R>(0.01));
   R us[3];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) us[d] = add_r(u[d], div_r(F[d], rs));
+  for (int d = 0; d < 3; ++d) us[d] = fma_r(F[d], inv_rs, u[d]);
   const R umag = sqrt_r(fma_r(us[0], us[0], fma_r(us[1], us[1], mul_r(us[2], us[2]))));
-  const R umax = umag > R(1e-10) ? umag : R(1e-10);
-  const R scale = div_r(R(0.25), umax);
-  if (scale < R(1)) {
+  if (umag > R(0.25)) {
+    const R scale = mul_r(R(0.25), rcp_r(umag));
 #pragma unroll
     for (int d = 0; d < 3; ++d) us[d] = mul_r(us[d], scale);
   }
@@ -201,7 +236,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   const R usq_b = fma_r(u[0], u[0], fma_r(u[1], u[1], mul_r(u[2], u[2])));
   const R usq_s = fma_r(us[0], us[0], fma_r(us[1], us[1], mul_r(us[2], us[2])));
   const R dusq = sub_r(usq_s, usq_b);
-  const R r36 = div_r(rho, R(36));
+  const R r36 = mul_r(rho, static_cast<R>(1.0 / 36.0));
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
     const R wr = mul_r(static_cast<R>(Lat<19>::wr(q)), r36);  // w_q rho
@@ -217,14 +252,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   }
   R* fo = static_cast<R*>(a.fout);
 #pragma unroll
-  for (int q = 0; q < 19; ++q) {
-    const uint32_t j0 = wrapu(static_cast<int>(x.i0) + Lat<19>::c0(q), g.n0);
-    const uint32_t j1 = wrapu(static_cast<int>(x.i1) + Lat<19>::c1(q), g.n1);
-    const uint32_t j2 = wrapu(static_cast<int>(x.k) + Lat<19>::c2(q), g.n2);
-    const uint32_t y = (j0 * g.n1 + j1) * g.n2 + j2;
-    const int slot = (wm != nullptr && __ldg(wm + y) != 0) ? Lat<19>::opp(q) : q;
-    fo[static_cast<size_t>(slot) * g.ncell + y] = f[q];
-  }
+  for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + nb(q)] = f[q];
 }
 
 }  // namespace lbm
