@@ -467,16 +467,16 @@ def pipe_cost(dev, steps=200):
     ``run`` (populations in and out in the reference layout):
     single phase (propeller 4e-4, gravity -1e-5, 70% fill) and Shan-Chen
     multiphase (G = -4.5, liquid 1.3 / gas 0.3, half filled).  Bytes per cell
-    and step of the passes as built: single phase 152 (D3Q19 step) + 12
-    (velocity for the tracer) + 12 + 56 (D3Q7 tracer step) = 232; multiphase
-    76 + 4 (density pass) + 76 + 4 + 76 (collide and push) = 236."""
+    and step of the passes as built: single phase 152 (D3Q19) + 56 (D3Q7
+    tracer) = 208 in one fused pass; multiphase 76 + 4 (density pass) + 76 + 4
+    + 76 (collide and push) = 236."""
     import torch
     from maddening_b200.pipe import LBMPipeNode
     out = {"workload": "384x192x192 pipe, FP32, %d steps" % steps}
     kw = dict(nx=384, ny=192, nz=192, tau=0.8, pipe_radius=0.9, propeller_x=96,
               propeller_radius=0.8, propeller_strength=4e-4, initial_velocity=0.005,
               gravity=-1e-5, tau_tracer=0.6)
-    modes = {"single_phase": (dict(fill_fraction=0.7), 232),
+    modes = {"single_phase": (dict(fill_fraction=0.7), 208),
              "multiphase": (dict(fill_fraction=0.5, G=-4.5, rho_liquid=1.3, rho_gas=0.3), 236)}
     for name, (extra, bpc) in modes.items():
         node = LBMPipeNode("bench_pipe", 1.0, device=dev, **kw, **extra)

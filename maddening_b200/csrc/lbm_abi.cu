@@ -984,6 +984,9 @@ size_t pipe_workspace(const lbm_plan* p) {
   return 2 * align256(state_bytes(p)) + 2 * align256(7 * n * p->io) + align256(3 * n * p->io);
 }
 
+// Single-phase pipe rollout: one fused launch per step (k_pipe_step: D3Q19
+// pull step + the tracer of the same cell), tracer populations ping-ponged
+// between two plane sets.
 template <class S>
 int run_pipe(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
              const void* t_in, void* t_out, int64_t n, double tau_tracer, void* tracer_out,
@@ -994,7 +997,6 @@ int run_pipe(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_i
   char* A = ws;
   char* B = ws + sb;
   char* T[2] = {ws + 2 * sb, ws + 2 * sb + tb};
-  char* U = ws + 2 * sb + 2 * tb;
   const unsigned grid = grid_for(p->g.ncell);
   lbm::TracerArgs t{};
   t.g = p->g;
@@ -1012,36 +1014,27 @@ int run_pipe(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_i
   rc = launch_prepare<19, S>(m, s);
   if (rc) return rc;
   int cur = 0;
-  auto tracer_step = [&](const void* vel) {
-    t.tin = T[cur];
-    t.tout = T[1 - cur];
-    t.vel = vel;
-    lbm::k_tracer_step<IO><<<grid, lbm::kBlock, 0, s>>>(t);
-    cur = 1 - cur;
-    return cuda_check(cudaGetLastError(), "k_tracer_step launch");
-  };
-  m.vel = U;  // each step's velocity (0 in walls) for the tracer
-  m.mflags = 0;
   for (int64_t i = 1; i < n; ++i) {
     m.pin = A;
     m.pout = B;
-    rc = launch_step<19, S>(m, false, s);
+    t.tin = T[cur];
+    t.tout = T[1 - cur];
+    lbm::k_pipe_step<S, false><<<grid, lbm::kBlock, 0, s>>>(m, t);
+    rc = cuda_check(cudaGetLastError(), "k_pipe_step launch");
     if (rc) return rc;
-    rc = tracer_step(U);
-    if (rc) return rc;
-    char* x = A;
-    A = B;
-    B = x;
+    cur = 1 - cur;
+    std::swap(A, B);
   }
   a.pin = A;
   a.f_out = f_out;
   a.prs = nullptr;
   a.mflags &= ~lbm::kMomRawVelocity;
-  if (a.vel == nullptr) a.vel = U;
-  rc = launch_step<19, S>(a, true, s);
+  t.tin = T[cur];
+  t.tout = T[1 - cur];
+  lbm::k_pipe_step<S, true><<<grid, lbm::kBlock, 0, s>>>(a, t);
+  rc = cuda_check(cudaGetLastError(), "k_pipe_step launch");
   if (rc) return rc;
-  rc = tracer_step(a.vel);
-  if (rc) return rc;
+  cur = 1 - cur;
   t.tin = T[cur];
   t.f7_out = t_out;
   t.tracer_out = tracer_out;

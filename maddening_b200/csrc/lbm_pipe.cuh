@@ -4,9 +4,10 @@
 //   new velocity, 0 in walls);  g_post = g in walls, else g - (g - g_eq)/tau_t;
 //   g_str = periodic shift by e_q;  g_bc = where(wall, g_str[opp], g_str);
 //   tracer_out = sum g_bc (0 in walls).
-// The collision needs the velocity of the same step at the same cell, which
-// the D3Q19 pass writes first, so the tracer runs as its own pass in push
-// form: a cell collides its own populations and sends population q to
+// The collision needs the velocity of the same step at the same cell: the
+// D3Q19 pull step has it in registers once it has taken the moments of f_bc,
+// so k_pipe_step runs the tracer of the cell in the same thread, in push
+// form: the cell collides its own populations and sends population q to
 // y = x + e_q, into slot opp(q) when y is a wall (the wall swap taken at the
 // destination; every slot is written exactly once).  Populations are FP32
 // (FP64 with FP64 plans), one plane per direction.
@@ -30,7 +31,6 @@ struct TracerArgs {
   const uint8_t* wall;
   const void* tin;      // populations (7 planes)
   void* tout;
-  const void* vel;      // (grid, 3) velocity of this step, 0 in walls
   double inv_tau;       // 1 / tau_tracer
   const void* f7_in;    // (grid, 7) reference layout (prepare)
   void* f7_out;         // (grid, 7) reference layout (final)
@@ -46,23 +46,20 @@ __global__ void __launch_bounds__(kBlock) k_tracer_prepare(const TracerArgs a) {
   for (int q = 0; q < 7; ++q) static_cast<IO*>(a.tout)[static_cast<size_t>(q) * a.g.ncell + c] = fi[q];
 }
 
+// Tracer step of cell x with this step's velocity uu (0 in walls).
 template <class IO>
-__global__ void __launch_bounds__(kBlock) k_tracer_step(const TracerArgs a) {
+__device__ __forceinline__ void tracer_cell(const TracerArgs& a, const Cell& x, bool wall,
+                                            const IO (&uu)[3]) {
   const Geo& g = a.g;
-  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= g.ncell) return;
-  const Cell x = locate(g, c);
+  const uint32_t c = x.c;
   const IO* tin = static_cast<const IO*>(a.tin);
   IO t[7];
 #pragma unroll
   for (int q = 0; q < 7; ++q) t[q] = tin[static_cast<size_t>(q) * g.ncell + c];
-  const bool wall = a.wall != nullptr && a.wall[c] != 0;
   if (!wall) {
     IO tracer = t[0];
 #pragma unroll
     for (int q = 1; q < 7; ++q) tracer = add_r(tracer, t[q]);
-    const IO* u = static_cast<const IO*>(a.vel) + static_cast<size_t>(c) * 3;
-    const IO uu[3] = {u[0], u[1], u[2]};
     const IO it = static_cast<IO>(a.inv_tau);
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
@@ -85,6 +82,43 @@ __global__ void __launch_bounds__(kBlock) k_tracer_step(const TracerArgs a) {
     const int slot = wy ? Lat7::opp(q) : q;
     tout[static_cast<size_t>(slot) * g.ncell + y] = t[q];
   }
+}
+
+// One pipe-node step of cell x: the D3Q19 pull step with the pipe force
+// (force mode 3: no half-force step in the moments), then the tracer step of
+// the same cell with the velocity just taken (lbm_pipe.py:751-879).  LAST
+// writes f_bc in the reference layout and the moment outputs instead of
+// colliding.
+template <class S, bool LAST>
+__global__ void __launch_bounds__(kBlock, min_blocks<S>())
+    k_pipe_step(const __grid_constant__ StepArgs a, const __grid_constant__ TracerArgs t) {
+  using R = typename StoreT<S>::R;
+  using IO = typename StoreT<S>::IO;
+  const uint32_t cidx = blockIdx.x * kBlock + threadIdx.x;
+  if (cidx >= a.g.ncell) return;
+  const Cell x = locate(a.g, cidx);
+  R d[19];
+  pull_cell<19, S>(a, x, d);
+  const bool wall = a.wall != nullptr && __ldg(a.wall + cidx) != 0;
+  R F[3];
+  pipe_force<R>(a, cidx, wall, F);
+  apply_bc<19, S, false>(a, x, wall, d);
+  const Mom<R> m = moments<19, R, true>(d, F, false);
+  if (LAST) {
+    store_moments<19, IO>(a, cidx, m, wall);
+    IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(cidx) * 19;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) fo[q] = static_cast<IO>(from_offset<19, R>(d[q], q));
+  } else {
+    collide<19, R, true>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
+#pragma unroll
+    for (int q = 0; q < 19; ++q)
+      static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * a.g.pstride + x.srow + x.k] =
+          from_r<S>(d[q]);
+  }
+  const IO uu[3] = {wall ? IO(0) : static_cast<IO>(m.u[0]), wall ? IO(0) : static_cast<IO>(m.u[1]),
+                    wall ? IO(0) : static_cast<IO>(m.u[2])};
+  tracer_cell<IO>(t, x, wall, uu);
 }
 
 // Last pass: populations to the reference layout and the tracer field.
