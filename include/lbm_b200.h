@@ -335,6 +335,30 @@ int lbm_reduce_workspace_bytes(const lbm_plan* plan, size_t* bytes);
 int lbm_mass_momentum(const lbm_plan* plan, lbm_stream_t stream, const void* f,
                       double* out_dev, void* workspace, size_t workspace_bytes);
 
+/* ---- Streaming frames ------------------------------------------------------
+ * The float payload of a streaming frame, MADDENING BinaryStateEncoder.encode
+ * (src/maddening/api/binary_encoder.py:151-205): each field (a contiguous
+ * device array) converted to float32, round to nearest, and written to
+ * out[offset .. offset + count), all fields in one launch.  The frame header
+ * (sim_time, 8 bytes) and any host-side fields are the caller's. */
+#define LBM_DTYPE_F32 0
+#define LBM_DTYPE_F16 1
+#define LBM_DTYPE_BF16 2
+#define LBM_DTYPE_F64 3
+#define LBM_DTYPE_U8 4  /* also bool */
+#define LBM_DTYPE_I32 5
+#define LBM_DTYPE_I64 6
+
+typedef struct {
+  const void* data; /* device pointer                         */
+  int64_t count;    /* elements                               */
+  int64_t offset;   /* first payload element written          */
+  int32_t dtype;    /* LBM_DTYPE_*                            */
+} lbm_pack_field;
+
+int lbm_pack_f32(lbm_stream_t stream, const lbm_pack_field* fields, int32_t n_fields,
+                 float* out, int64_t out_count);
+
 #ifdef __cplusplus
 }
 #endif

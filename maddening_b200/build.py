@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "liblbm_b200.so"
 SOURCES = ["lbm_abi.cu"]
 HEADERS = ["lbm_kernels.cuh", "lbm_lattice.cuh", "lbm_adjoint.cuh", "lbm_staged.cuh",
-           "lbm_pair.cuh", "lbm_pipe.cuh", "lbm_multiphase.cuh"]
+           "lbm_pair.cuh", "lbm_pipe.cuh", "lbm_multiphase.cuh", "lbm_pack.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",

@@ -16,6 +16,7 @@
 #include "lbm_kernels.cuh"
 #include "lbm_pair.cuh"
 #include "lbm_multiphase.cuh"
+#include "lbm_pack.cuh"
 #include "lbm_pipe.cuh"
 #include "lbm_staged.cuh"
 
@@ -1569,6 +1570,47 @@ int lbm_mass_momentum(const lbm_plan* p, lbm_stream_t stream, const void* f, dou
     }
   }
   return cuda_check(cudaGetLastError(), "k_mass_momentum launch");
+}
+
+int lbm_pack_f32(lbm_stream_t stream, const lbm_pack_field* fields, int32_t n_fields,
+                 float* out, int64_t out_count) {
+  if (n_fields < 0) return fail(LBM_ERR_INVALID, "n_fields must be >= 0 (got %d)", n_fields);
+  if (n_fields > 0 && fields == nullptr) return fail(LBM_ERR_INVALID, "fields is NULL");
+  int64_t total = 0;
+  for (int32_t i = 0; i < n_fields; ++i) {
+    const lbm_pack_field& f = fields[i];
+    if (f.count < 0) return fail(LBM_ERR_INVALID, "field %d: count %lld < 0", i, (long long)f.count);
+    if (f.offset < 0) return fail(LBM_ERR_INVALID, "field %d: offset %lld < 0", i, (long long)f.offset);
+    if (f.count > 0 && f.data == nullptr) return fail(LBM_ERR_INVALID, "field %d: data is NULL", i);
+    if (f.dtype < LBM_DTYPE_F32 || f.dtype > LBM_DTYPE_I64)
+      return fail(LBM_ERR_INVALID, "field %d: unknown dtype %d", i, f.dtype);
+    if (f.offset + f.count > out_count)
+      return fail(LBM_ERR_INVALID, "field %d: elements [%lld, %lld) outside the payload of %lld",
+                  i, (long long)f.offset, (long long)(f.offset + f.count), (long long)out_count);
+    total += f.count;
+  }
+  if (total > 0 && out == nullptr) return fail(LBM_ERR_INVALID, "out is NULL");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  for (int32_t first = 0; first < n_fields; first += lbm::kPackMaxFields) {
+    const int32_t nb = std::min<int32_t>(lbm::kPackMaxFields, n_fields - first);
+    lbm::PackBatch b{};
+    int64_t most = 0;
+    for (int32_t j = 0; j < nb; ++j) {
+      const lbm_pack_field& f = fields[first + j];
+      b.src[j] = f.data;
+      b.count[j] = f.count;
+      b.offset[j] = f.offset;
+      b.type[j] = f.dtype;
+      most = std::max(most, f.count);
+    }
+    if (most == 0) continue;
+    const int64_t want = (most + lbm::kPackThreads - 1) / lbm::kPackThreads;
+    const unsigned gx = static_cast<unsigned>(std::min<int64_t>(want, 148 * 8));
+    lbm::k_pack_f32<<<dim3(gx, nb), lbm::kPackThreads, 0, s>>>(b, out);
+    const int rc = cuda_check(cudaGetLastError(), "k_pack_f32 launch");
+    if (rc) return rc;
+  }
+  return LBM_OK;
 }
 
 }  // extern "C"

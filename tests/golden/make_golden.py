@@ -160,7 +160,7 @@ def _install_shims(ref_root: Path):
     src = ref_root / "src"
     sys.path.insert(0, str(src))
     import maddening  # noqa: F401  (lazy __init__, no jax import)
-    for pkg in ("maddening.core", "maddening.nodes"):
+    for pkg in ("maddening.core", "maddening.nodes", "maddening.api"):
         mod = types.ModuleType(pkg)
         mod.__path__ = [str(src / Path(*pkg.split(".")))]
         sys.modules[pkg] = mod
@@ -438,6 +438,67 @@ def run_pipe_case(pipe, jnp, case, mode):
     return out
 
 
+TRANSFORM_SCALES = [(1e-3, 1e-6, 1060.0), (2.5e-5, 3e-7, 998.2), (0.01, 0.02, 1.2)]
+
+
+def transform_vectors(tu):
+    """core/transforms_unit.py: each factory applied to a ramp, and its name."""
+    x = np.linspace(-2.0, 3.0, 11)
+    out = {}
+    for i, (dx, dt, rho) in enumerate(TRANSFORM_SCALES):
+        made = {"lbm_to_si_force": tu.lbm_to_si_force(dx, dt, rho),
+                "si_to_lbm_force": tu.si_to_lbm_force(dx, dt, rho),
+                "lbm_to_si_torque": tu.lbm_to_si_torque(dx, dt, rho),
+                "lbm_to_si_velocity": tu.lbm_to_si_velocity(dx, dt),
+                "lbm_to_si_pressure": tu.lbm_to_si_pressure(dx, dt, rho),
+                "lbm_to_si_length": tu.lbm_to_si_length(dx)}
+        for name, fn in made.items():
+            out[f"transform|{i}|{name}|values"] = np.asarray(fn(x))
+            out[f"transform|{i}|{name}|qualname"] = np.array(fn.__qualname__)
+    out["transform|input"] = x
+    return out
+
+
+def frame_states():
+    """States for the streaming-frame fixtures: the shape of the reference's
+    own encoder test (scalars and a 20-cell rod) and a mixed-dtype lattice
+    state (float32 populations, float64 density, float16 velocity, uint8 wall
+    mask, int64 counter, Python scalar)."""
+    rng = np.random.default_rng(11)
+    grid = (4, 3, 5)
+    return {
+        "rods": {"ball": {"position": np.array(5.0, dtype=np.float32),
+                          "velocity": np.array(-3.2, dtype=np.float32)},
+                 "heat_rod": {"temperature": np.ones(20, dtype=np.float32) * 20.0},
+                 "table": {"position": np.array(0.0, dtype=np.float32)}},
+        "lattice": {"vessel": {"f": rng.random(grid + (19,)).astype(np.float32),
+                               "density": 1.0 + 1e-3 * rng.standard_normal(grid),
+                               "velocity": (0.05 * rng.standard_normal(grid + (3,))).astype(np.float16),
+                               "wall_mask": (rng.random(grid) < 0.3).astype(np.uint8),
+                               "steps": np.arange(6, dtype=np.int64) * 1000003},
+                    "heart": {"pressure": np.array(13.25), "volume": 71.5}},
+    }
+
+
+FRAME_SUBSCRIPTIONS = {"all": None, "subset": {"vessel": ["velocity", "density", "nope"],
+                                               "heart": ["volume"], "missing": ["x"]},
+                       "nothing": {}}
+
+
+def frame_vectors(be):
+    """api/binary_encoder.py: schema and frame bytes of each state and subscription."""
+    import json
+    out = {}
+    for sname, state in frame_states().items():
+        for subname, sub in FRAME_SUBSCRIPTIONS.items():
+            enc = be.BinaryStateEncoder(state, fields=sub)
+            frame = enc.encode(0.125 * len(sname), state)
+            key = f"frame|{sname}|{subname}"
+            out[key + "|bytes"] = np.frombuffer(frame, dtype=np.uint8).copy()
+            out[key + "|schema"] = np.array(json.dumps(enc.schema()))
+    return out
+
+
 def unit_vectors(lbm, jnp, seed=7):
     """Golden vectors for the pure kernels on random inputs (x64)."""
     rng = np.random.default_rng(seed)
@@ -503,6 +564,8 @@ def main(ref_root="/root/reference"):
             for k, v in res.items():
                 golden[f"{case['name']}|{mode}|{k}"] = v
     MODE["value"] = "x64"
+    golden.update(transform_vectors(importlib.import_module("maddening.core.transforms_unit")))
+    golden.update(frame_vectors(importlib.import_module("maddening.api.binary_encoder")))
     out = Path(__file__).with_name("lbm_golden.npz")
     np.savez_compressed(out, **golden)
     meta = {c["name"]: c for c in CASES + PADDED_CASES + PIPE_CASES}
