@@ -452,6 +452,45 @@ constexpr int batched_min_blocks() { return sizeof(typename StoreT<S>::R) == 8 ?
 // the reference f and the moments of this step (a recorded history step).
 enum StepMode : int { kOutState = 0, kOutAoS = 1, kOutMoments = 2, kOutRecord = 3 };
 
+// ---------------------------------------------------------------------------
+// Block-staged stores to the reference layout (*grid, Q)
+// ---------------------------------------------------------------------------
+// The kBlock cells of a block are consecutive, so their Q values each form one
+// contiguous run of the output.  Written directly, thread t's values sit Q
+// elements apart from thread t+1's and every store instruction of a warp
+// touches 32 separate sectors; staged here, the block writes the run with
+// 16-byte stores.  Thread t of the block owns row t of the tile.
+template <int Q, class IO>
+__device__ __forceinline__ IO* aos_tile() {
+  __shared__ __align__(16) IO tile[kBlock * Q];
+  return tile;
+}
+
+// Writes the tile rows of cells [first, min(first + kBlock, ncell)) to
+// out[first * Q ...].  Every thread of the block must call it (it holds the
+// barriers on both sides, so the tile can be refilled afterwards).
+template <int Q, class IO>
+__device__ __forceinline__ void aos_flush(IO* out, uint32_t first, uint32_t ncell) {
+  const IO* tile = aos_tile<Q, IO>();
+  __syncthreads();
+  if (first < ncell) {
+    const uint32_t cells = ncell - first < static_cast<uint32_t>(kBlock) ? ncell - first : kBlock;
+    const uint32_t n = cells * Q;
+    IO* dst = out + static_cast<size_t>(first) * Q;
+    uint32_t done = 0;
+    if ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+      constexpr uint32_t V = 16 / sizeof(IO);
+      const uint32_t nv = n / V;
+      const uint4* src4 = reinterpret_cast<const uint4*>(tile);
+      uint4* dst4 = reinterpret_cast<uint4*>(dst);
+      for (uint32_t i = threadIdx.x; i < nv; i += kBlock) dst4[i] = src4[i];
+      done = nv * V;
+    }
+    for (uint32_t i = done + threadIdx.x; i < n; i += kBlock) dst[i] = tile[i];
+  }
+  __syncthreads();
+}
+
 struct Cell {
   uint32_t c;      // linear cell index (reference layout)
   uint32_t i0, i1, k;
@@ -633,10 +672,11 @@ __device__ __forceinline__ void finish_cell(const StepArgs& a, const Cell& x,
   store_moments<Q, IO>(a, cidx, m, wall);
 
   if constexpr (MODE == kOutAoS || MODE == kOutRecord) {
+    // f_bc into this thread's tile row; the kernel writes the block's run
     if (MODE == kOutAoS || a.f_out != nullptr) {
-      IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(cidx) * Q;
+      IO* row = aos_tile<Q, IO>() + threadIdx.x * Q;
 #pragma unroll
-      for (int q = 0; q < Q; ++q) fo[q] = static_cast<IO>(from_offset<Q, R>(d[q], q));
+      for (int q = 0; q < Q; ++q) row[q] = static_cast<IO>(from_offset<Q, R>(d[q], q));
     }
   }
   if constexpr (MODE == kOutState || MODE == kOutRecord) {
@@ -687,8 +727,13 @@ __device__ __forceinline__ void step_cell(const StepArgs& a, uint32_t cidx) {
 template <int Q, class S, int MODE, bool FACES, bool FORCE>
 __global__ void __launch_bounds__(kBlock, min_blocks<S>())
     k_step(const __grid_constant__ StepArgs a) {
+  using IO = typename StoreT<S>::IO;
   const uint32_t cidx = blockIdx.x * kBlock + threadIdx.x;
   if (cidx < a.g.ncell) step_cell<Q, S, MODE, FACES, FORCE>(a, cidx);
+  if constexpr (MODE == kOutAoS || MODE == kOutRecord) {
+    if (MODE == kOutAoS || a.f_out != nullptr)
+      aos_flush<Q, IO>(static_cast<IO*>(a.f_out), blockIdx.x * kBlock, a.g.ncell);
+  }
 }
 
 // Halo-padded block (the reference's update_padded, lbm.py:747-897): one halo
@@ -704,20 +749,22 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
   using IO = typename StoreT<S>::IO;
   const Geo& g = a.g;
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= g.ncell) return;
-  const Cell x = locate(g, c);
-  const bool halo = (Lat<Q>::D == 3 && (x.i0 == 0 || x.i0 == g.n0 - 1)) || x.i1 == 0 ||
-                    x.i1 == g.n1 - 1 || x.k == 0 || x.k == g.n2 - 1;
-  if (halo) {
-    const IO* fi = static_cast<const IO*>(a.f_in) + static_cast<size_t>(c) * Q;
-    IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(c) * Q;
+  if (c < g.ncell) {
+    const Cell x = locate(g, c);
+    const bool halo = (Lat<Q>::D == 3 && (x.i0 == 0 || x.i0 == g.n0 - 1)) || x.i1 == 0 ||
+                      x.i1 == g.n1 - 1 || x.k == 0 || x.k == g.n2 - 1;
+    if (halo) {
+      const IO* fi = static_cast<const IO*>(a.f_in) + static_cast<size_t>(c) * Q;
+      IO* row = aos_tile<Q, IO>() + threadIdx.x * Q;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) fo[q] = fi[q];
-    return;
+      for (int q = 0; q < Q; ++q) row[q] = fi[q];
+    } else {
+      R d[Q];
+      pull_cell<Q, S>(a, x, d);
+      finish_cell<Q, S, kOutAoS, FACES, FORCE>(a, x, d);
+    }
   }
-  R d[Q];
-  pull_cell<Q, S>(a, x, d);
-  finish_cell<Q, S, kOutAoS, FACES, FORCE>(a, x, d);
+  aos_flush<Q, IO>(static_cast<IO*>(a.f_out), blockIdx.x * kBlock, g.ncell);
 }
 
 // ---------------------------------------------------------------------------
@@ -796,10 +843,16 @@ __global__ void __launch_bounds__(kBlock, batched_min_blocks<S>())
 #endif
 #pragma unroll 1
     for (int j = 0; j < kBatchTile / kBlock; ++j) {
-      const uint32_t c = tile.first + j * kBlock + threadIdx.x;
-      if (c >= sa.g.ncell) break;
-      if constexpr (SPEC == 0) step_cell_any<Q, S, MODE>(sa, c);
-      else step_cell<Q, S, MODE, ((SPEC - 1) & 2) != 0, ((SPEC - 1) & 1) != 0>(sa, c);
+      const uint32_t first = tile.first + j * kBlock;  // block-uniform
+      if (first >= sa.g.ncell) break;
+      const uint32_t c = first + threadIdx.x;
+      if (c < sa.g.ncell) {
+        if constexpr (SPEC == 0) step_cell_any<Q, S, MODE>(sa, c);
+        else step_cell<Q, S, MODE, ((SPEC - 1) & 2) != 0, ((SPEC - 1) & 1) != 0>(sa, c);
+      }
+      if constexpr (MODE == kOutAoS)
+        aos_flush<Q, typename StoreT<S>::IO>(static_cast<typename StoreT<S>::IO*>(sa.f_out),
+                                             first, sa.g.ncell);
     }
   }
 }

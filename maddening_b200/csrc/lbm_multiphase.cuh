@@ -101,10 +101,8 @@ __device__ __forceinline__ R psi_of(R rho, R rho0) {
 }
 
 template <class R, int MODE>
-__global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
+__device__ __forceinline__ void density_cell(const MPArgs& a, uint32_t c) {
   const Geo& g = a.s.g;
-  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= g.ncell) return;
   R f[19];
   if (MODE == kMPFirst) {
     const R* fi = static_cast<const R*>(a.f_aos_in) + static_cast<size_t>(c) * 19;
@@ -142,14 +140,14 @@ __global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
 #pragma unroll
     for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + c] = f[q];
   }
-  if (MODE != kMPLast) {
+  if constexpr (MODE != kMPLast) {
     static_cast<R*>(a.psi)[c] =
         wall ? static_cast<R>(a.psi_wall) : psi_of(s, static_cast<R>(a.rho0));
     return;
   }
-  R* fo = static_cast<R*>(a.f_aos_out) + static_cast<size_t>(c) * 19;
+  R* row = aos_tile<19, R>() + threadIdx.x * 19;
 #pragma unroll
-  for (int q = 0; q < 19; ++q) fo[q] = f[q];
+  for (int q = 0; q < 19; ++q) row[q] = f[q];
   if (a.rho_out != nullptr) static_cast<R*>(a.rho_out)[c] = rho_out;
   if (a.vel_out != nullptr) {
     const R den = s0 > R(1e-10) ? s0 : R(1e-10);
@@ -161,6 +159,18 @@ __global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
     R t = div_r(sub_r(rho_out, static_cast<R>(a.rho_gas)), static_cast<R>(a.drho));
     t = t < R(0) ? R(0) : (t > R(1) ? R(1) : t);
     static_cast<R*>(a.tracer_out)[c] = wall ? R(0) : t;
+  }
+}
+
+template <class R, int MODE>
+__global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
+  const Geo& g = a.s.g;
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if constexpr (MODE == kMPLast) {  // every thread reaches the block's staged store
+    if (c < g.ncell) density_cell<R, MODE>(a, c);
+    aos_flush<19, R>(static_cast<R*>(a.f_aos_out), blockIdx.x * kBlock, g.ncell);
+  } else if (c < g.ncell) {
+    density_cell<R, MODE>(a, c);
   }
 }
 

@@ -95,50 +95,55 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
   const uint32_t cidx = blockIdx.x * kBlock + threadIdx.x;
-  if (cidx >= a.g.ncell) return;
-  const Cell x = locate(a.g, cidx);
-  R d[19];
-  pull_cell<19, S>(a, x, d);
-  const bool wall = a.wall != nullptr && __ldg(a.wall + cidx) != 0;
-  R F[3];
-  pipe_force<R>(a, cidx, wall, F);
-  apply_bc<19, S, false>(a, x, wall, d);
-  const Mom<R> m = moments<19, R, true>(d, F, false);
-  if (LAST) {
-    store_moments<19, IO>(a, cidx, m, wall);
-    IO* fo = static_cast<IO*>(a.f_out) + static_cast<size_t>(cidx) * 19;
+  if (cidx < a.g.ncell) {
+    const Cell x = locate(a.g, cidx);
+    R d[19];
+    pull_cell<19, S>(a, x, d);
+    const bool wall = a.wall != nullptr && __ldg(a.wall + cidx) != 0;
+    R F[3];
+    pipe_force<R>(a, cidx, wall, F);
+    apply_bc<19, S, false>(a, x, wall, d);
+    const Mom<R> m = moments<19, R, true>(d, F, false);
+    if (LAST) {
+      store_moments<19, IO>(a, cidx, m, wall);
+      IO* row = aos_tile<19, IO>() + threadIdx.x * 19;
 #pragma unroll
-    for (int q = 0; q < 19; ++q) fo[q] = static_cast<IO>(from_offset<19, R>(d[q], q));
-  } else {
-    collide<19, R, true>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
+      for (int q = 0; q < 19; ++q) row[q] = static_cast<IO>(from_offset<19, R>(d[q], q));
+    } else {
+      collide<19, R, true>(d, m, F, static_cast<R>(a.omega), static_cast<R>(a.guo_c));
 #pragma unroll
-    for (int q = 0; q < 19; ++q)
-      static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * a.g.pstride + x.srow + x.k] =
-          from_r<S>(d[q]);
+      for (int q = 0; q < 19; ++q)
+        static_cast<S*>(a.pout)[static_cast<uint32_t>(q) * a.g.pstride + x.srow + x.k] =
+            from_r<S>(d[q]);
+    }
+    const IO uu[3] = {wall ? IO(0) : static_cast<IO>(m.u[0]),
+                      wall ? IO(0) : static_cast<IO>(m.u[1]),
+                      wall ? IO(0) : static_cast<IO>(m.u[2])};
+    tracer_cell<IO>(t, x, wall, uu);
   }
-  const IO uu[3] = {wall ? IO(0) : static_cast<IO>(m.u[0]), wall ? IO(0) : static_cast<IO>(m.u[1]),
-                    wall ? IO(0) : static_cast<IO>(m.u[2])};
-  tracer_cell<IO>(t, x, wall, uu);
+  if (LAST) aos_flush<19, IO>(static_cast<IO*>(a.f_out), blockIdx.x * kBlock, a.g.ncell);
 }
 
 // Last pass: populations to the reference layout and the tracer field.
 template <class IO>
 __global__ void __launch_bounds__(kBlock) k_tracer_final(const TracerArgs a) {
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= a.g.ncell) return;
-  const IO* tin = static_cast<const IO*>(a.tin);
-  IO* fo = static_cast<IO*>(a.f7_out) + static_cast<size_t>(c) * 7;
-  IO s = 0;
+  if (c < a.g.ncell) {
+    const IO* tin = static_cast<const IO*>(a.tin);
+    IO* row = aos_tile<7, IO>() + threadIdx.x * 7;
+    IO s = 0;
 #pragma unroll
-  for (int q = 0; q < 7; ++q) {
-    const IO v = tin[static_cast<size_t>(q) * a.g.ncell + c];
-    fo[q] = v;
-    s = q == 0 ? v : add_r(s, v);
+    for (int q = 0; q < 7; ++q) {
+      const IO v = tin[static_cast<size_t>(q) * a.g.ncell + c];
+      row[q] = v;
+      s = q == 0 ? v : add_r(s, v);
+    }
+    if (a.tracer_out != nullptr) {
+      const bool wall = a.wall != nullptr && a.wall[c] != 0;
+      static_cast<IO*>(a.tracer_out)[c] = wall ? IO(0) : s;
+    }
   }
-  if (a.tracer_out != nullptr) {
-    const bool wall = a.wall != nullptr && a.wall[c] != 0;
-    static_cast<IO*>(a.tracer_out)[c] = wall ? IO(0) : s;
-  }
+  aos_flush<7, IO>(static_cast<IO*>(a.f7_out), blockIdx.x * kBlock, a.g.ncell);
 }
 
 }  // namespace lbm
