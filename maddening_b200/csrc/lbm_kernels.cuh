@@ -491,6 +491,33 @@ __device__ __forceinline__ void aos_flush(IO* out, uint32_t first, uint32_t ncel
   __syncthreads();
 }
 
+// Reads the values of cells [first, min(first + kBlock, ncell)) from
+// in[first * Q ...] into the tile (16-byte loads when aligned); afterwards
+// thread t finds its cell's Q values in tile row t.  Every thread of the
+// block must call it.
+template <int Q, class IO>
+__device__ __forceinline__ const IO* aos_fill(const IO* in, uint32_t first, uint32_t ncell) {
+  IO* tile = aos_tile<Q, IO>();
+  __syncthreads();  // an earlier use of the tile is over
+  if (first < ncell) {
+    const uint32_t cells = ncell - first < static_cast<uint32_t>(kBlock) ? ncell - first : kBlock;
+    const uint32_t n = cells * Q;
+    const IO* src = in + static_cast<size_t>(first) * Q;
+    uint32_t done = 0;
+    if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+      constexpr uint32_t V = 16 / sizeof(IO);
+      const uint32_t nv = n / V;
+      const uint4* src4 = reinterpret_cast<const uint4*>(src);
+      uint4* dst4 = reinterpret_cast<uint4*>(tile);
+      for (uint32_t i = threadIdx.x; i < nv; i += kBlock) dst4[i] = __ldg(src4 + i);
+      done = nv * V;
+    }
+    for (uint32_t i = done + threadIdx.x; i < n; i += kBlock) tile[i] = __ldg(src + i);
+  }
+  __syncthreads();
+  return tile + threadIdx.x * Q;
+}
+
 struct Cell {
   uint32_t c;      // linear cell index (reference layout)
   uint32_t i0, i1, k;
@@ -569,17 +596,18 @@ __device__ __forceinline__ R from_offset(R d, int q) {
 
 // Collide from a reference-layout state f (*grid_shape, Q): p = C(f).
 // Cell-local; the first pass of every update / rollout.
+// fi: the cell's Q reference values (a tile row filled by aos_fill).
 template <int Q, class S, bool FORCE>
-__device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
+__device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c,
+                                             const typename StoreT<S>::IO* fi) {
   using R = typename StoreT<S>::R;
   using IO = typename StoreT<S>::IO;
   // index in the state planes (differs only for padded rows)
   const uint32_t ci =
       a.g.rstride == a.g.n2 ? c : c + fdiv(c, a.g.div_n2) * (a.g.rstride - a.g.n2);
-  const IO* fi = static_cast<const IO*>(a.f_in) + static_cast<size_t>(c) * Q;
   R d[Q];
 #pragma unroll
-  for (int q = 0; q < Q; ++q) d[q] = to_offset<Q, R>(static_cast<R>(__ldg(fi + q)), q);
+  for (int q = 0; q < Q; ++q) d[q] = to_offset<Q, R>(static_cast<R>(fi[q]), q);
   R F[3] = {0, 0, 0};
   if (FORCE) {
     if (a.force_mode == 2) load_force<Q, IO>(a.force_field, c, F);
@@ -598,8 +626,10 @@ __device__ __forceinline__ void prepare_cell(const StepArgs& a, uint32_t c) {
 template <int Q, class S, bool FORCE>
 __global__ void __launch_bounds__(kBlock, min_blocks<S>())
     k_prepare(const __grid_constant__ StepArgs a) {
+  using IO = typename StoreT<S>::IO;
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c < a.g.ncell) prepare_cell<Q, S, FORCE>(a, c);
+  const IO* row = aos_fill<Q, IO>(static_cast<const IO*>(a.f_in), blockIdx.x * kBlock, a.g.ncell);
+  if (c < a.g.ncell) prepare_cell<Q, S, FORCE>(a, c, row);
 }
 
 // Wall-node swap (lbm.py:944-948): a wall cell takes f_str[..., opp].
@@ -873,10 +903,14 @@ __global__ void __launch_bounds__(kBlock, batched_min_blocks<S>())
     }
 #pragma unroll 1
     for (int j = 0; j < kBatchTile / kBlock; ++j) {
-      const uint32_t c = tile.first + j * kBlock + threadIdx.x;
+      const uint32_t first = tile.first + j * kBlock;  // block-uniform
+      if (first >= sa.g.ncell) break;
+      const uint32_t c = first + threadIdx.x;
+      using IO = typename StoreT<S>::IO;
+      const IO* row = aos_fill<Q, IO>(static_cast<const IO*>(sa.f_in), first, sa.g.ncell);
       if (c < sa.g.ncell) {
-        if (sa.force_mode != 0) prepare_cell<Q, S, true>(sa, c);
-        else prepare_cell<Q, S, false>(sa, c);
+        if (sa.force_mode != 0) prepare_cell<Q, S, true>(sa, c, row);
+        else prepare_cell<Q, S, false>(sa, c, row);
       }
     }
   }

@@ -100,14 +100,14 @@ __device__ __forceinline__ R psi_of(R rho, R rho0) {
   return mul_r(rho0, -expm1_r(div_r(-rho, rho0)));
 }
 
+// row: the cell's reference values (first pass; a tile row filled by aos_fill).
 template <class R, int MODE>
-__device__ __forceinline__ void density_cell(const MPArgs& a, uint32_t c) {
+__device__ __forceinline__ void density_cell(const MPArgs& a, uint32_t c, const R* row) {
   const Geo& g = a.s.g;
   R f[19];
   if (MODE == kMPFirst) {
-    const R* fi = static_cast<const R*>(a.f_aos_in) + static_cast<size_t>(c) * 19;
 #pragma unroll
-    for (int q = 0; q < 19; ++q) f[q] = fi[q];
+    for (int q = 0; q < 19; ++q) f[q] = row[q];
   } else {
     const R* fi = static_cast<const R*>(a.fin);
 #pragma unroll
@@ -145,9 +145,9 @@ __device__ __forceinline__ void density_cell(const MPArgs& a, uint32_t c) {
         wall ? static_cast<R>(a.psi_wall) : psi_of(s, static_cast<R>(a.rho0));
     return;
   }
-  R* row = aos_tile<19, R>() + threadIdx.x * 19;
+  R* out_row = aos_tile<19, R>() + threadIdx.x * 19;
 #pragma unroll
-  for (int q = 0; q < 19; ++q) row[q] = f[q];
+  for (int q = 0; q < 19; ++q) out_row[q] = f[q];
   if (a.rho_out != nullptr) static_cast<R*>(a.rho_out)[c] = rho_out;
   if (a.vel_out != nullptr) {
     const R den = s0 > R(1e-10) ? s0 : R(1e-10);
@@ -166,11 +166,16 @@ template <class R, int MODE>
 __global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
   const Geo& g = a.s.g;
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if constexpr (MODE == kMPLast) {  // every thread reaches the block's staged store
-    if (c < g.ncell) density_cell<R, MODE>(a, c);
+  // the first and last passes stage the reference layout: every thread of
+  // the block reaches the tile's barriers
+  if constexpr (MODE == kMPLast) {
+    if (c < g.ncell) density_cell<R, MODE>(a, c, nullptr);
     aos_flush<19, R>(static_cast<R*>(a.f_aos_out), blockIdx.x * kBlock, g.ncell);
+  } else if constexpr (MODE == kMPFirst) {
+    const R* row = aos_fill<19, R>(static_cast<const R*>(a.f_aos_in), blockIdx.x * kBlock, g.ncell);
+    if (c < g.ncell) density_cell<R, MODE>(a, c, row);
   } else if (c < g.ncell) {
-    density_cell<R, MODE>(a, c);
+    density_cell<R, MODE>(a, c, nullptr);
   }
 }
 

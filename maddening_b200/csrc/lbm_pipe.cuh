@@ -40,8 +40,8 @@ struct TracerArgs {
 template <class IO>
 __global__ void __launch_bounds__(kBlock) k_tracer_prepare(const TracerArgs a) {
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  const IO* fi = aos_fill<7, IO>(static_cast<const IO*>(a.f7_in), blockIdx.x * kBlock, a.g.ncell);
   if (c >= a.g.ncell) return;
-  const IO* fi = static_cast<const IO*>(a.f7_in) + static_cast<size_t>(c) * 7;
 #pragma unroll
   for (int q = 0; q < 7; ++q) static_cast<IO*>(a.tout)[static_cast<size_t>(q) * a.g.ncell + c] = fi[q];
 }

@@ -1,8 +1,9 @@
-"""Reference-layout outputs (*grid, Q) are written block by block through
-shared memory with 16-byte stores when the output is 16-byte aligned, and
-with plain coalesced stores otherwise.  Both give the same bytes: a rollout
-written to an output shifted by one element (so never 16-byte aligned) equals
-the aligned one, on lattices whose cell count leaves a partial last block."""
+"""Reference-layout inputs and outputs (*grid, Q) move block by block through
+shared memory, with 16-byte loads and stores when the array is 16-byte
+aligned and plain coalesced ones otherwise.  Both give the same bytes: a
+rollout read from and written to arrays shifted by one element (so never
+16-byte aligned) equals the aligned one, on lattices whose cell count leaves
+a partial last block."""
 
 import ctypes as C
 
@@ -36,9 +37,13 @@ def test_unaligned_output_equals_aligned(shape, lattice, storage):
     big = torch.full((n + 1,), float("nan"), dtype=st["f"].dtype, device=dev)
     f_out = big[1:]  # one element past a 256-byte boundary
     assert f_out.data_ptr() % 16 != 0
+    big_in = torch.empty((n + 1,), dtype=st["f"].dtype, device=dev)
+    f_in = big_in[1:]
+    f_in.copy_(st["f"].reshape(-1))
+    assert f_in.data_ptr() % 16 != 0
     ws = torch.empty(node.plan.workspace_bytes(), dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
-    _lib.check(_lib.lib().lbm_rollout(node.plan.handle, stream, st["f"].data_ptr(),
+    _lib.check(_lib.lib().lbm_rollout(node.plan.handle, stream, f_in.data_ptr(),
                                       f_out.data_ptr(), 5, C.byref(args), C.byref(mom),
                                       ws.data_ptr(), ws.numel()))
     torch.cuda.synchronize()
