@@ -315,6 +315,10 @@ def run_ours(args):
         variants["batched"] = batched_cost(dev)
         torch.cuda.empty_cache()
         variants["pipe"] = pipe_cost(dev)
+        torch.cuda.empty_cache()
+        variants["update_call"] = update_call_cost(dev)
+        torch.cuda.empty_cache()
+        variants["frames"] = frames_cost(dev)
 
     if rank == 0:
         peak, peak_kind = _peaks()
@@ -461,9 +465,9 @@ def batched_cost(dev, steps=500):
     return out
 
 
-def pipe_cost(dev, steps=200):
+def pipe_cost(dev, steps=200, grid=(384, 192, 192)):
     """The pipe node (LBMPipeNode) on a 384 x 192 x 192 pipe (14.2 M cells,
-    radius 0.9, propeller disc at x = 96), FP32, best of three K-step runs of
+    radius 0.9, propeller disc at x = nx / 4), FP32, best of three K-step runs of
     ``run`` (populations in and out in the reference layout):
     single phase (propeller 4e-4, gravity -1e-5, 70% fill) and Shan-Chen
     multiphase (G = -4.5, liquid 1.3 / gas 0.3, half filled).  Bytes per cell
@@ -472,8 +476,9 @@ def pipe_cost(dev, steps=200):
     + 76 (collide and push) = 236."""
     import torch
     from maddening_b200.pipe import LBMPipeNode
-    out = {"workload": "384x192x192 pipe, FP32, %d steps" % steps}
-    kw = dict(nx=384, ny=192, nz=192, tau=0.8, pipe_radius=0.9, propeller_x=96,
+    nx, ny, nz = grid
+    out = {"workload": "%dx%dx%d pipe, FP32, %d steps" % (nx, ny, nz, steps)}
+    kw = dict(nx=nx, ny=ny, nz=nz, tau=0.8, pipe_radius=0.9, propeller_x=nx // 4,
               propeller_radius=0.8, propeller_strength=4e-4, initial_velocity=0.005,
               gravity=-1e-5, tau_tracer=0.6)
     modes = {"single_phase": (dict(fill_fraction=0.7), 208),
@@ -492,13 +497,84 @@ def pipe_cost(dev, steps=200):
             e1.record()
             torch.cuda.synchronize()
             best = min(best, e0.elapsed_time(e1) / 1e3)
-        cells = 384 * 192 * 192
+        cells = nx * ny * nz
         m = cells * steps / best / 1e6
         out[name] = {"mlups": round(m, 1), "bytes_per_cell": bpc,
                      "hbm_frac": round(m * 1e6 * bpc / 1e9 / _peaks()[0], 4)}
         del node, st
         torch.cuda.empty_cache()
     return out
+
+
+def update_call_cost(dev, grid=(256, 256, 256), calls=20):
+    """One ``LBMNode.update`` call per step, as a graph manager drives the node:
+    the reference-layout state in and out of every call (a prepare pass and a
+    last pass), on the benchmark workload; mean over ``calls`` calls."""
+    import torch
+    from maddening_b200 import LBMNode
+    from maddening_b200.geometry import random_spheres
+    node = LBMNode("call", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0,
+                   wall_mask=random_spheres(grid, seed=0), outlet_condition="zero_gradient",
+                   device=dev)
+    bi = {"inlet_velocity": np.array(U_IN)}
+    st = node.initial_state()
+    for _ in range(3):
+        st = node.update(st, bi, 1.0)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(calls):
+        st = node.update(st, bi, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    cells = grid[0] * grid[1] * grid[2]
+    return {"workload": "LBMNode.update, one call per step, %s" % "x".join(map(str, grid)),
+            "ms_per_call": round(ms, 4), "mlups": round(cells / ms / 1e3, 1),
+            "bytes_per_cell": 324,
+            "hbm_frac": round(cells * 324 / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
+
+
+def frames_cost(dev, grid=(256, 256, 256), frames=20):
+    """Streaming frames of a running node (BinaryStateEncoder over density and
+    velocity of the benchmark lattice, 16 B per cell): the one-launch device
+    gather alone (encode_device) and whole frames to host bytes (encode)."""
+    import torch
+    from maddening_b200 import LBMNode
+    from maddening_b200.streaming import BinaryStateEncoder
+    node = LBMNode("frames", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0, device=dev)
+    st = node.run(node.initial_state(), {"body_force": np.array([1e-6, 0.0, 0.0])}, 3)
+    state = {"vessel": st}
+    enc = BinaryStateEncoder(state, fields={"vessel": ["density", "velocity"]})
+    enc.encode(0.0, state)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(frames):
+        enc.encode_device(state)
+    e1.record()
+    torch.cuda.synchronize()
+    t_pack = e0.elapsed_time(e1) / frames / 1e3
+    t0 = time.perf_counter()
+    for i in range(frames):
+        frame = enc.encode(float(i), state)
+    t_frame = (time.perf_counter() - t0) / frames
+    t0 = time.perf_counter()
+    for i in range(frames):
+        enc.encode_view(float(i), state)
+    t_view = (time.perf_counter() - t0) / frames
+    payload = enc.total_floats * 4
+    return {"workload": "frames of density + velocity, %s lattice" % "x".join(map(str, grid)),
+            "frame_bytes": len(frame), "pack_ms": round(t_pack * 1e3, 4),
+            "pack_hbm_frac": round(2 * payload / t_pack / 1e9 / _peaks()[0], 4),
+            "frame_ms": round(t_frame * 1e3, 3),
+            "frame_gbs": round(len(frame) / t_frame / 1e9, 2),
+            "view_ms": round(t_view * 1e3, 3),
+            "view_gbs": round(len(frame) / t_view / 1e9, 2),
+            "note": "frame: pack + one device-to-host copy into the pinned frame buffer + one "
+                    "copy into bytes; view: the same without the bytes copy"}
 
 
 def adjoint_cost(dev):
@@ -586,11 +662,26 @@ def main():
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
     ap.add_argument("--c5-steps", type=int, default=2000,
                     help="steps of the 512^3 precision comparison (variants)")
+    ap.add_argument("--only", choices=["pipe", "update_call", "frames"],
+                    help="run one variant alone and print its JSON (for profiling)")
+    ap.add_argument("--variant-grid", default=None,
+                    help="lattice of --only, e.g. 192x128x128 (default: the variant's own)")
     args = ap.parse_args()
     global GRID
     GRID = (args.grid,) * 3
     if args.warmup < 3:
         args.warmup = 3
+    if args.only:
+        import torch
+        dev = torch.device("cuda", 0)
+        kw = {}
+        if args.variant_grid:
+            kw["grid"] = tuple(int(v) for v in args.variant_grid.split("x"))
+        fn = {"pipe": pipe_cost, "update_call": update_call_cost, "frames": frames_cost}[args.only]
+        if args.only == "pipe":
+            kw["steps"] = args.steps
+        print(json.dumps({args.only: fn(dev, **kw)}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

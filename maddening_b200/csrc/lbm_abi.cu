@@ -350,10 +350,10 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   char* B = ws + sb;
   a.f_in = f_in;
   a.pout = A;
-  int rc = launch_prepare<Q, S>(a, s);
-  if (rc) return rc;
-  lbm::StepArgs m = a;  // intermediate steps write no moments
+  lbm::StepArgs m = a;  // the first pass and intermediate steps write no moments
   m.rho = m.vel = m.prs = nullptr;
+  int rc = launch_prepare<Q, S>(m, s);
+  if (rc) return rc;
   // The bulk copies need 16-byte aligned rows: the caller's workspace too.
   const bool staged = n > 1 && staged_ok<Q, S>(p) && reinterpret_cast<uintptr_t>(ws) % 16 == 0;
   if (staged) {
@@ -1604,7 +1604,7 @@ int lbm_pack_f32(lbm_stream_t stream, const lbm_pack_field* fields, int32_t n_fi
       most = std::max(most, f.count);
     }
     if (most == 0) continue;
-    const int64_t want = (most + lbm::kPackThreads - 1) / lbm::kPackThreads;
+    const int64_t want = (most + 4 * lbm::kPackThreads - 1) / (4 * lbm::kPackThreads);
     const unsigned gx = static_cast<unsigned>(std::min<int64_t>(want, 148 * 8));
     lbm::k_pack_f32<<<dim3(gx, nb), lbm::kPackThreads, 0, s>>>(b, out);
     const int rc = cuda_check(cudaGetLastError(), "k_pack_f32 launch");

@@ -48,9 +48,19 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_f32(const __grid_constant
   const int32_t type = b.type[f];
   float* dst = out + b.offset[f];
   const int64_t stride = static_cast<int64_t>(gridDim.x) * kPackThreads;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * kPackThreads + threadIdx.x; i < n;
-       i += stride)
-    dst[i] = pack_value(src, type, i);
+  int64_t i = static_cast<int64_t>(blockIdx.x) * kPackThreads + threadIdx.x;
+  // four independent loads in flight per thread, then the remainder
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    const float v0 = pack_value(src, type, i);
+    const float v1 = pack_value(src, type, i + stride);
+    const float v2 = pack_value(src, type, i + 2 * stride);
+    const float v3 = pack_value(src, type, i + 3 * stride);
+    dst[i] = v0;
+    dst[i + stride] = v1;
+    dst[i + 2 * stride] = v2;
+    dst[i + 3 * stride] = v3;
+  }
+  for (; i < n; i += stride) dst[i] = pack_value(src, type, i);
 }
 
 }  // namespace lbm

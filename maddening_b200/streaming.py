@@ -12,8 +12,10 @@ converted to float32 and gathered into one device payload by a single
 ``lbm_pack_f32`` launch, then copied to pinned host memory in one transfer;
 the state itself (e.g. a (grid, 19) population array) never crosses to the
 host unless it is subscribed.  Host values (NumPy arrays, Python scalars, CPU
-tensors) are written on the host.  ``encode_device`` returns the payload as a
-device tensor for consumers on the GPU.
+tensors) are written on the host.  A frame is assembled in one pinned host
+buffer; ``encode`` copies it once into the returned bytes, ``encode_view``
+hands out a view of the buffer itself, and ``encode_device`` returns the
+payload as a device tensor for consumers on the GPU.
 
 Compression (``"zstd"``, ``"zstd+xor"``) follows the reference and needs the
 ``zstandard`` package; without it the constructor raises ``ImportError``.
@@ -102,7 +104,7 @@ class BinaryStateEncoder:
                 self._total_floats += n
         self._buf_size = 8 + self._total_floats * 4
         self._dev_payload: dict[torch.device, torch.Tensor] = {}
-        self._host_payload: torch.Tensor | None = None
+        self._frame: torch.Tensor | None = None
 
     # -- schema ---------------------------------------------------------------
     def schema(self) -> dict:
@@ -175,24 +177,27 @@ class BinaryStateEncoder:
         (device, items), = dev.items()
         return self._pack_on(device, items)[: self._total_floats]
 
-    def _payload(self, state) -> bytes:
-        nbytes = self._total_floats * 4
-        if nbytes == 0:
-            return b""
+    def _fill_frame(self, sim_time: float, state) -> np.ndarray:
+        """The uncompressed frame in the encoder's own (pinned) host buffer:
+        ``[8 B sim_time][payload]``, as a uint8 array over that buffer."""
+        if self._frame is None:
+            self._frame = torch.empty(self._buf_size, dtype=torch.uint8,
+                                      pin_memory=torch.cuda.is_available())
+        frame = self._frame.numpy()
+        struct.pack_into("d", frame, 0, sim_time)
+        if self._total_floats == 0:
+            return frame
+        payload = self._frame[8:].view(torch.float32)
         dev, host = self._split(state)
-        if self._host_payload is None:
-            self._host_payload = torch.empty(self._total_floats, dtype=torch.float32,
-                                             pin_memory=torch.cuda.is_available())
-        hp = self._host_payload
         for device, items in dev.items():
             buf = self._pack_on(device, items)
             if len(dev) == 1:  # one transfer; host fields are written over it below
-                hp.copy_(buf[: self._total_floats], non_blocking=True)
+                payload.copy_(buf[: self._total_floats], non_blocking=True)
             else:
                 for _val, offset, n in items:
-                    hp[offset: offset + n].copy_(buf[offset: offset + n], non_blocking=True)
+                    payload[offset: offset + n].copy_(buf[offset: offset + n], non_blocking=True)
             torch.cuda.current_stream(device).synchronize()
-        out = hp.numpy()
+        out = payload.numpy()
         for val, offset, n in host:
             if isinstance(val, torch.Tensor):
                 val = val.detach().numpy()
@@ -200,15 +205,25 @@ class BinaryStateEncoder:
                 out[offset: offset + n] = np.asarray(val.flatten(), dtype=np.float32)
             else:
                 out[offset] = np.float32(float(val))
-        return out.tobytes()
+        return frame
+
+    def encode_view(self, sim_time: float, state: dict) -> memoryview:
+        """The uncompressed frame without a host-side copy: a view of the
+        encoder's pinned frame buffer, valid until the next encode call (for
+        senders that take a buffer, e.g. a WebSocket ``send_bytes``)."""
+        if self._compression != "none":
+            raise ValueError("encode_view gives uncompressed frames; use encode")
+        return memoryview(self._fill_frame(sim_time, state))
 
     def encode(self, sim_time: float, state: dict) -> bytes:
         """``[8 B sim_time][payload]``, the payload compressed when asked
-        (binary_encoder.py:151-205)."""
-        payload = self._payload(state)
+        (binary_encoder.py:151-205).  Uncompressed, the frame is assembled in
+        the pinned buffer and copied once into the returned bytes."""
+        frame = self._fill_frame(sim_time, state)
         if self._compression == "none":
-            wire = payload
-        elif self._compression == "zstd":
+            return frame.tobytes()
+        payload = frame[8:].tobytes()
+        if self._compression == "zstd":
             wire = self._cctx.compress(payload)
         else:  # zstd+xor: XOR against the previous payload, then compress
             if self._prev_payload is None or len(self._prev_payload) != len(payload):

@@ -97,3 +97,10 @@ def test_compression_modes(sample_state):
             BinaryStateEncoder(sample_state, compression="zstd")
     with pytest.raises(NotImplementedError):
         decode_frame(b"\0" * 8, {"compression": "zstd+xor"})
+
+
+def test_encode_view_is_the_frame(sample_state):
+    enc = BinaryStateEncoder(sample_state)
+    view = enc.encode_view(1.25, sample_state)
+    assert bytes(view) == enc.encode(1.25, sample_state)
+    assert len(view) == enc.frame_bytes
