@@ -191,17 +191,26 @@ def _barrier(world):
     import torch.distributed as dist
     if world > 1:
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def _max_over_ranks(world, value):
+    """The largest ``value`` of all ranks (device timings: the job's time)."""
     import torch
     import torch.distributed as dist
     if world == 1:
         return value
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def _job_mlups(world, cells, steps, t_max):
+    """Whole-job throughput of ``world`` replicas of ``cells`` x ``steps``
+    lattice updates, timed as the slowest rank's ``t_max`` seconds."""
+    return world * cells * steps / t_max / 1e6
 
 
 def run_ours(args):
@@ -253,7 +262,7 @@ def run_ours(args):
         _barrier(world)
     t_dev = e0.elapsed_time(e1) / 1e3
     t_dev = _max_over_ranks(world, t_dev)
-    mlups = world * cells * K / t_dev / 1e6
+    mlups = _job_mlups(world, cells, K, t_dev)
     clocks = clk.summary()
 
     # e2e: public API, state in pinned host memory
@@ -344,7 +353,7 @@ def run_ours(args):
                          "bytes_per_cell": bytes_per_cell,
                          "kernel": "k_step<19,float,0,true,false> (fused pull-stream-collide, "
                                    "faces on)"},
-            "e2e": {"value": round(world * cells * K / t_e2e / 1e6, 1), "unit": "MLUPS",
+            "e2e": {"value": round(_job_mlups(world, cells, K, t_e2e), 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
                     "note": "LBMNode.run with pinned-host state in/out, per K-step rollout"},
             "gpu_launches": K + 1,
