@@ -155,6 +155,8 @@ class BinaryStateEncoder:
         if buf is None:
             buf = torch.empty(max(1, self._total_floats), dtype=torch.float32, device=device)
             self._dev_payload[device] = buf
+        # keep: contiguous / converted copies stay referenced until the launch
+        # is queued (the caching allocator orders any reuse on this stream)
         keep, descs = [], []
         for val, offset, n in items:
             t = val.contiguous()
@@ -170,7 +172,8 @@ class BinaryStateEncoder:
 
     def encode_device(self, state: dict) -> torch.Tensor:
         """The float32 payload as a device tensor (all subscribed fields must
-        live on one CUDA device)."""
+        live on one CUDA device).  It is the encoder's own buffer: valid until
+        the next encode call on that device."""
         dev, host = self._split(state)
         if host or len(dev) != 1:
             raise ValueError("encode_device needs every subscribed field on one CUDA device")
