@@ -1,0 +1,73 @@
+"""Properties of the step at the benchmark's full size (256^3, 16.8 M cells),
+where no CPU oracle finishes: they hold for any lattice size, so the oracle
+checks at small sizes carry over.
+
+* translation equivariance: on a periodic lattice, shifting the state and the
+  walls commutes with the rollout, bit for bit (every cell runs the same
+  arithmetic on the same neighbour values), one-cell FP32 and paired FP16;
+* mass: walls and a uniform force conserve sum(rho) (FP64 reduction);
+* momentum: without walls a uniform force F raises sum(f e) by exactly N F per
+  step (the Guo source adds (1 - omega/2) F, the half-force moments return
+  omega F / 2)."""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+GRID = (256, 256, 256)
+N = GRID[0] * GRID[1] * GRID[2]
+
+
+def _state(node, seed):
+    rng = np.random.default_rng(seed)
+    st = node.initial_state()
+    w = node.lattice.w
+    f = torch.as_tensor(w, dtype=torch.float32, device="cuda").expand(GRID + (19,)).clone()
+    noise = torch.as_tensor(rng.standard_normal((64, 64, 64, 19)).astype(np.float32),
+                            device="cuda").repeat(4, 4, 4, 1)
+    st["f"] = f * (1 + 1e-3 * noise)
+    return st
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_translation_equivariance(storage):
+    from maddening_b200 import LBMNode
+    wall = np.random.default_rng(1).random(GRID) < 0.05
+    shift = (5, 17, 3)
+    kw = dict(grid_shape=GRID, viscosity=0.05, storage=storage)
+    a = LBMNode("a", 1.0, wall_mask=wall, **kw)
+    b = LBMNode("b", 1.0, wall_mask=np.roll(wall, shift, axis=(0, 1, 2)), **kw)
+    st = _state(a, 2)
+    bi = {"body_force": np.array([2e-6, -1e-6, 5e-7], dtype=np.float32)}
+    ra = a.run(st, bi, 60)
+    sb = dict(st, f=torch.roll(st["f"], shift, dims=(0, 1, 2)))
+    sb.pop("wall_mask", None)
+    rb = b.run(sb, bi, 60)
+    for key in ("f", "density", "velocity", "pressure"):
+        assert torch.equal(rb[key], torch.roll(ra[key], shift, dims=(0, 1, 2))), key
+
+
+def test_mass_conserved_with_walls():
+    from maddening_b200 import LBMNode
+    wall = np.random.default_rng(3).random(GRID) < 0.05
+    node = LBMNode("m", 1.0, grid_shape=GRID, viscosity=0.05, wall_mask=wall)
+    st = _state(node, 4)
+    m0 = node.mass_momentum(st["f"])[0].item()
+    out = node.run(st, {"body_force": np.array([1e-5, 0.0, 0.0], dtype=np.float32)}, 200)
+    m1 = node.mass_momentum(out["f"])[0].item()
+    assert abs(m1 - m0) <= 1e-7 * m0, (m0, m1)
+
+
+def test_momentum_balance_without_walls():
+    from maddening_b200 import LBMNode
+    node = LBMNode("p", 1.0, grid_shape=GRID, viscosity=0.05)
+    st = _state(node, 5)
+    F = np.array([1e-5, -4e-6, 2e-6])
+    steps = 200
+    j0 = node.mass_momentum(st["f"])[1:].cpu().numpy()
+    out = node.run(st, {"body_force": F.astype(np.float32)}, steps)
+    j1 = node.mass_momentum(out["f"])[1:].cpu().numpy()
+    expect = steps * N * F.astype(np.float32).astype(np.float64)
+    np.testing.assert_allclose(j1 - j0, expect, rtol=1e-5, atol=0)
