@@ -325,6 +325,8 @@ def run_ours(args):
         torch.cuda.empty_cache()
         variants["pipe"] = pipe_cost(dev)
         torch.cuda.empty_cache()
+        variants["d2q9"] = d2q9_cost(dev)
+        torch.cuda.empty_cache()
         variants["update_call"] = update_call_cost(dev)
         torch.cuda.empty_cache()
         variants["frames"] = frames_cost(dev)
@@ -515,6 +517,41 @@ def pipe_cost(dev, steps=200, grid=(384, 192, 192)):
     return out
 
 
+def d2q9_cost(dev, grid=(4096, 4096), steps=500):
+    """D2Q9 channel: 4096 x 4096 (16.8 M cells), walls on the two y rows,
+    periodic x, uniform force 1e-6 along x, tau 0.6; FP32 (72 B per cell and
+    step) and FP16 offsets (36 B); best of three K-step rollouts."""
+    import torch
+    from maddening_b200 import LBMNode
+    wall = np.zeros(grid, dtype=bool)
+    wall[:, 0] = wall[:, -1] = True
+    bi = {"body_force": np.array([1e-6, 0.0], dtype=np.float32)}
+    cells = grid[0] * grid[1]
+    out = {"workload": "%dx%d D2Q9 channel, %d steps" % (grid[0], grid[1], steps)}
+    for storage, bpc in (("f32", 72), ("f16", 36)):
+        node = LBMNode("d2", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0, lattice="D2Q9",
+                       wall_mask=wall, storage=storage, device=dev)
+        st = node.initial_state()
+        node.run(st, bi, 3)
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            node.run(st, bi, steps)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        m = cells * steps / best / 1e6
+        out[storage] = {"mlups": round(m, 1), "bytes_per_cell": bpc,
+                        "hbm_frac": round(m * 1e6 * bpc / 1e9 / _peaks()[0], 4)}
+        del node, st
+        torch.cuda.empty_cache()
+    out["f16_over_f32"] = round(out["f16"]["mlups"] / out["f32"]["mlups"], 3)
+    return out
+
+
 def update_call_cost(dev, grid=(256, 256, 256), calls=20):
     """One ``LBMNode.update`` call per step, as a graph manager drives the node:
     the reference-layout state in and out of every call (a prepare pass and a
@@ -671,7 +708,7 @@ def main():
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
     ap.add_argument("--c5-steps", type=int, default=2000,
                     help="steps of the 512^3 precision comparison (variants)")
-    ap.add_argument("--only", choices=["pipe", "update_call", "frames"],
+    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9"],
                     help="run one variant alone and print its JSON (for profiling)")
     ap.add_argument("--variant-grid", default=None,
                     help="lattice of --only, e.g. 192x128x128 (default: the variant's own)")
@@ -686,7 +723,8 @@ def main():
         kw = {}
         if args.variant_grid:
             kw["grid"] = tuple(int(v) for v in args.variant_grid.split("x"))
-        fn = {"pipe": pipe_cost, "update_call": update_call_cost, "frames": frames_cost}[args.only]
+        fn = {"pipe": pipe_cost, "update_call": update_call_cost, "frames": frames_cost,
+              "d2q9": d2q9_cost}[args.only]
         if args.only == "pipe":
             kw["steps"] = args.steps
         print(json.dumps({args.only: fn(dev, **kw)}), flush=True)
