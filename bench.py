@@ -327,6 +327,8 @@ def run_ours(args):
         torch.cuda.empty_cache()
         variants["d2q9"] = d2q9_cost(dev)
         torch.cuda.empty_cache()
+        variants["c1"] = c1_cost(dev)
+        torch.cuda.empty_cache()
         variants["update_call"] = update_call_cost(dev)
         torch.cuda.empty_cache()
         variants["frames"] = frames_cost(dev)
@@ -552,6 +554,59 @@ def d2q9_cost(dev, grid=(4096, 4096), steps=500):
     return out
 
 
+def c1_cost(dev, grid=(64, 64, 64), steps=500):
+    """The 64^3 channel (z walls, periodic x and y, tau 0.8, body force 1e-6 x,
+    FP32), 500 steps: a rollout as queued launches, and the same rollout
+    captured once in a CUDA graph and replayed.  Its 40 MB of state stay in the
+    126 MB L2, so the HBM fraction is indicative only; launch gaps dominate."""
+    import torch
+    from maddening_b200 import LBMNode
+    wall = np.zeros(grid, dtype=bool)
+    wall[:, :, 0] = wall[:, :, -1] = True
+    node = LBMNode("c1", 1.0, grid_shape=grid, viscosity=0.1, wall_mask=wall, device=dev)
+    bi = {"body_force": np.array([1e-6, 0.0, 0.0], dtype=np.float32)}
+    st = node.initial_state()
+    cells = grid[0] * grid[1] * grid[2]
+
+    def timed(fn):
+        best = float("inf")
+        for _ in range(5):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        return cells * steps / best / 1e6
+
+    node.run(st, bi, 3)
+    torch.cuda.synchronize()
+    plain = timed(lambda: node.run(st, bi, steps))
+    out = {"workload": "64^3 channel, z walls, force, FP32, %d steps" % steps,
+           "queued_mlups": round(plain, 1)}
+    try:
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            node.run(st, bi, steps)
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            node.run(st, bi, steps)
+        g.replay()
+        torch.cuda.synchronize()
+        out["graph_mlups"] = round(timed(g.replay), 1)
+        del g
+    except Exception as exc:  # capture needs no host sync inside run
+        out["graph_mlups"] = None
+        out["graph_error"] = str(exc)[:200]
+    out["bytes_per_cell"] = 152
+    best = max(v for v in (out["queued_mlups"], out.get("graph_mlups") or 0))
+    out["hbm_frac_indicative"] = round(best * 1e6 * 152 / 1e9 / _peaks()[0], 4)
+    return out
+
+
 def update_call_cost(dev, grid=(256, 256, 256), calls=20):
     """One ``LBMNode.update`` call per step, as a graph manager drives the node:
     the reference-layout state in and out of every call (a prepare pass and a
@@ -708,7 +763,7 @@ def main():
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
     ap.add_argument("--c5-steps", type=int, default=2000,
                     help="steps of the 512^3 precision comparison (variants)")
-    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9"],
+    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9", "c1"],
                     help="run one variant alone and print its JSON (for profiling)")
     ap.add_argument("--variant-grid", default=None,
                     help="lattice of --only, e.g. 192x128x128 (default: the variant's own)")
@@ -724,7 +779,7 @@ def main():
         if args.variant_grid:
             kw["grid"] = tuple(int(v) for v in args.variant_grid.split("x"))
         fn = {"pipe": pipe_cost, "update_call": update_call_cost, "frames": frames_cost,
-              "d2q9": d2q9_cost}[args.only]
+              "d2q9": d2q9_cost, "c1": c1_cost}[args.only]
         if args.only == "pipe":
             kw["steps"] = args.steps
         print(json.dumps({args.only: fn(dev, **kw)}), flush=True)
