@@ -268,6 +268,30 @@ void launch_pair_w(const lbm::StepArgs& a, cudaStream_t s) {
   }
 }
 
+template <int Q, class S, int W>
+void launch_quad_w(const lbm::StepArgs& a, cudaStream_t s) {
+  const dim3 grid(a.g.n0 * a.g.n1, a.g.n2 / (128 * W));
+  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
+  const bool force = a.force_mode != 0;
+  if (faces) {
+    if (force) lbm::k_step_quad<Q, S, true, true, W><<<grid, 32 * W, 0, s>>>(a);
+    else lbm::k_step_quad<Q, S, true, false, W><<<grid, 32 * W, 0, s>>>(a);
+  } else {
+    if (force) lbm::k_step_quad<Q, S, false, true, W><<<grid, 32 * W, 0, s>>>(a);
+    else lbm::k_step_quad<Q, S, false, false, W><<<grid, 32 * W, 0, s>>>(a);
+  }
+}
+
+// The four-cell form (D2Q9, 16-bit storage): rows of a multiple of 128 cells,
+// unpadded state rows, 8-byte aligned planes and a 4-byte aligned wall mask.
+template <int Q, class S>
+bool quad_ok(const lbm::StepArgs& a) {
+  return Q == 9 && sizeof(S) == 2 && a.g.n2 % 128 == 0 && a.g.rstride == a.g.n2 &&
+         a.g.pstride % 4 == 0 && reinterpret_cast<uintptr_t>(a.pin) % 8 == 0 &&
+         reinterpret_cast<uintptr_t>(a.pout) % 8 == 0 &&
+         reinterpret_cast<uintptr_t>(a.wall) % 4 == 0;
+}
+
 template <int Q, class S>
 void launch_gpair(const lbm::StepArgs& a, cudaStream_t s) {
   const unsigned grid = grid_for(a.g.ncell / 2);
@@ -287,6 +311,14 @@ int launch_pair(const lbm::StepArgs& a, cudaStream_t s) {
   if constexpr (sizeof(S) == 8) {
     return fail(LBM_ERR_UNSUPPORTED, "paired step has no FP64 form");
   } else {
+    if constexpr (Q == 9 && sizeof(S) == 2) {
+      if (quad_ok<Q, S>(a)) {
+        if (a.g.n2 % 512 == 0) launch_quad_w<Q, S, 4>(a, s);
+        else if (a.g.n2 % 256 == 0) launch_quad_w<Q, S, 2>(a, s);
+        else launch_quad_w<Q, S, 1>(a, s);
+        return cuda_check(cudaGetLastError(), "k_step_quad launch");
+      }
+    }
     if (a.g.n2 % 256 == 0) launch_pair_w<Q, S, 4>(a, s);
     else if (a.g.n2 % 128 == 0) launch_pair_w<Q, S, 2>(a, s);
     else if (a.g.n2 % 64 == 0) launch_pair_w<Q, S, 1>(a, s);

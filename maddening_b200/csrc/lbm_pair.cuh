@@ -236,6 +236,127 @@ __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
   pair_finish<Q, S, FACES, FORCE, false>(a, i0, i1, k, row * g.n2, row * g.rstride, v, e, true);
 }
 
+// ---------------------------------------------------------------------------
+// Four cells per thread (D2Q9, 16-bit storage)
+// ---------------------------------------------------------------------------
+// A D2Q9 cell carries 9 x 2 B, so a pair still leaves each thread with few
+// bytes in flight and a large share of per-cell overhead (addresses, memory
+// instructions, the wall load, the vote).  Here lane l of a warp owns cells
+// k..k+3 (k = first + 4 l) of one row and moves each plane as one 64-bit word
+// (four 16-bit offsets); the pull along the row takes the neighbour of cell k
+// (c2 = +1) or of cell k+3 (c2 = -1) from the aligned 32-bit word before /
+// after the quad.  Every cell then runs the one-cell arithmetic (bit-identical
+// results).  Block: W warps = 128 W consecutive cells of one row; rows of a
+// multiple of 128 W cells.
+template <class S>
+struct QuadT {
+  static __device__ __forceinline__ uint2 ld(const S* p) {
+    return __ldg(reinterpret_cast<const uint2*>(p));
+  }
+  static __device__ __forceinline__ void st(S* p, float a, float b, float c, float d) {
+    uint2 w;
+    PairT<S>::st(reinterpret_cast<S*>(&w.x), a, b);
+    PairT<S>::st(reinterpret_cast<S*>(&w.y), c, d);
+    *reinterpret_cast<uint2*>(p) = w;
+  }
+};
+
+template <int Q, class S, bool FACES, bool FORCE, int W>
+__global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
+    k_step_quad(const __grid_constant__ StepArgs a) {
+  using PT = PairT<S>;
+  const Geo& g = a.g;
+  const uint32_t row = blockIdx.x;
+  const uint32_t i0 = fdiv(row, g.div_n1);
+  const uint32_t i1 = row - i0 * g.n1;
+  const uint32_t k = blockIdx.y * (128u * W) + 4u * threadIdx.x;
+  const uint32_t kprev = (k == 0 ? g.n2 : k) - 2u;       // word holding cell k - 1 (high)
+  const uint32_t knext = k + 4u == g.n2 ? 0u : k + 4u;  // word holding cell k + 4 (low)
+  const uint32_t i0m = i0 == 0 ? g.n0 - 1 : i0 - 1, i0p = i0 + 1 == g.n0 ? 0u : i0 + 1;
+  const uint32_t i1m = i1 == 0 ? g.n1 - 1 : i1 - 1, i1p = i1 + 1 == g.n1 ? 0u : i1 + 1;
+  const S* pin = static_cast<const S*>(a.pin);
+  float d[4][Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
+    const uint32_t s0 = c0 > 0 ? i0m : (c0 < 0 ? i0p : i0);
+    const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
+    const S* base = pin + (static_cast<uint32_t>(q) * g.pstride + (s0 * g.n1 + s1) * g.rstride);
+    const uint2 v = QuadT<S>::ld(base + k);
+    if (c2 == 0) {
+      d[0][q] = PT::lo(v.x);
+      d[1][q] = PT::hi(v.x);
+      d[2][q] = PT::lo(v.y);
+      d[3][q] = PT::hi(v.y);
+    } else if (c2 > 0) {  // cell j pulls j - 1
+      d[0][q] = PT::hi(PT::ld(base + kprev));
+      d[1][q] = PT::lo(v.x);
+      d[2][q] = PT::hi(v.x);
+      d[3][q] = PT::lo(v.y);
+    } else {  // cell j pulls j + 1
+      d[0][q] = PT::hi(v.x);
+      d[1][q] = PT::lo(v.y);
+      d[2][q] = PT::hi(v.y);
+      d[3][q] = PT::lo(PT::ld(base + knext));
+    }
+  }
+  const uint32_t rbase = row * g.n2;
+  bool w[4] = {false, false, false, false};
+  if (a.wall != nullptr) {
+    const uint32_t w4 = __ldg(reinterpret_cast<const unsigned int*>(a.wall + rbase + k));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[j] = ((w4 >> (8 * j)) & 0xffu) != 0;
+  }
+  if (__any_sync(0xffffffffu, w[0] || w[1] || w[2] || w[3])) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (w[j]) wall_swap<Q>(d[j]);
+  }
+  if constexpr (FACES) {
+    bool near = false;
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+      const FaceK& fc = a.face[fi];
+      if (fc.kind == kFaceNone) continue;
+      const uint32_t ins = a.face_inset;
+      if (fc.axis == 0) near |= i0 == (fc.side == 0 ? ins : g.n0 - 1 - ins);
+      else if (fc.axis == 1) near |= i1 == (fc.side == 0 ? ins : g.n1 - 1 - ins);
+      else near |= (fc.side == 0 ? ins : g.n2 - 1 - ins) - k <= 3u;  // one of k..k+3
+    }
+    if (near) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (w[j]) continue;
+        Cell x;
+        x.c = rbase + k + j;
+        x.i0 = i0;
+        x.i1 = i1;
+        x.k = k + j;
+        x.row = rbase;
+        x.srow = row * g.rstride;
+        apply_faces<Q, S>(a, x, d[j]);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    Cell x;
+    x.c = rbase + k + j;
+    x.i0 = i0;
+    x.i1 = i1;
+    x.k = k + j;
+    x.row = rbase;
+    x.srow = row * g.rstride;
+    pair_cell<Q, S, FORCE>(a, x, d[j]);
+  }
+  S* pout = static_cast<S*>(a.pout);
+  const uint32_t sbase = row * g.rstride;
+#pragma unroll
+  for (int q = 0; q < Q; ++q)
+    QuadT<S>::st(pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k), d[0][q], d[1][q],
+                 d[2][q], d[3][q]);
+}
+
 // Pairs of the state planes' index: pair j holds state cells 2j, 2j + 1 (rows
 // of even length -- padded ones included -- so a pair never spans two rows).
 // Row coordinates and source rows are per lane.  PAD: padded state rows.

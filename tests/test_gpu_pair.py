@@ -4,7 +4,8 @@ the one-cell step for every storage form, lattice, face axis and force mode,
 including the periodic wrap at both ends of a row and every warp/block width
 (contiguous extents 64, 128, 192, 256); the instance-wide pair form for other
 even rows (rows shorter than a warp, pairs whose neighbour lies in the next
-row, a partial last warp); odd rows fall back to the one-cell step."""
+row, a partial last warp); the four-cell form of D2Q9 16-bit storage (rows of
+128, 256, 384, 512 cells); odd rows fall back to the one-cell step."""
 
 import numpy as np
 import pytest
@@ -51,6 +52,8 @@ def _node(shape, storage, lattice, kind, cpt, seed=0):
 @pytest.mark.parametrize("shape,lattice", [((6, 5, 64), "D3Q19"), ((4, 3, 256), "D3Q19"),
                                            ((3, 4, 128), "D3Q19"), ((5, 2, 192), "D3Q19"),
                                            ((1, 1, 64), "D3Q19"), ((40, 128), "D2Q9"),
+                                           ((24, 256), "D2Q9"), ((9, 512), "D2Q9"),
+                                           ((7, 384), "D2Q9"),
                                            # instance-wide pairs (even rows)
                                            ((3, 4, 100), "D3Q19"), ((5, 3, 34), "D3Q19"),
                                            ((4, 7, 2), "D3Q19"), ((33, 38), "D2Q9"),
