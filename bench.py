@@ -57,6 +57,14 @@ BYTES_PER_CELL = 152  # D3Q19 FP32: 19 x 4 B read + 19 x 4 B written
 # algorithmic (the remainder of the writes is still in L2 when the launch ends).
 NCU_TRAFFIC_256_F32 = 2.51e9
 METRIC = "MLUPS (D3Q19 FP32 lattice updates/s) & HBM roofline fraction"
+# the state-step kernel each storage form runs on the workload (rows of 256 cells)
+KERNEL_LABEL = {
+    "f32": "k_step<19,float,kOutState,faces,no force> (fused pull-stream-collide, one cell "
+           "per thread)",
+    "f64": "k_step<19,double,kOutState,faces,no force> (one cell per thread)",
+    "f16": "k_step_quad<19,__half,faces,no force,2> (four cells per thread, 64-bit words)",
+    "bf16": "k_step_quad<19,__nv_bfloat16,faces,no force,2> (four cells per thread)",
+}
 WORKLOAD = "256^3 D3Q19 obstacle flow, velocity inlet + zero-gradient outlet, tau 0.6"
 
 
@@ -355,8 +363,7 @@ def run_ours(args):
                          "traffic_unit": "DRAM bytes per launch (ncu)",
                          "algorithmic_bytes_per_launch": bytes_per_cell * cells,
                          "bytes_per_cell": bytes_per_cell,
-                         "kernel": "k_step<19,float,0,true,false> (fused pull-stream-collide, "
-                                   "faces on)"},
+                         "kernel": KERNEL_LABEL[args.storage]},
             "e2e": {"value": round(_job_mlups(world, cells, K, t_e2e), 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
                     "note": "LBMNode.run with pinned-host state in/out, per K-step rollout"},

@@ -237,11 +237,11 @@ __global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
 }
 
 // ---------------------------------------------------------------------------
-// Four cells per thread (D2Q9, 16-bit storage)
+// Four cells per thread (16-bit storage)
 // ---------------------------------------------------------------------------
-// A D2Q9 cell carries 9 x 2 B, so a pair still leaves each thread with few
-// bytes in flight and a large share of per-cell overhead (addresses, memory
-// instructions, the wall load, the vote).  Here lane l of a warp owns cells
+// With 16-bit offsets a pair still leaves each thread with few bytes in
+// flight and a large share of per-cell overhead (addresses, memory
+// instructions, the wall load, the vote): a D2Q9 cell carries only 9 x 2 B.  Here lane l of a warp owns cells
 // k..k+3 (k = first + 4 l) of one row and moves each plane as one 64-bit word
 // (four 16-bit offsets); the pull along the row takes the neighbour of cell k
 // (c2 = +1) or of cell k+3 (c2 = -1) from the aligned 32-bit word before /
@@ -261,8 +261,16 @@ struct QuadT {
   }
 };
 
+// Resident warps the D3Q19 four-cell budget is set for (sweep 16 / 20 / 24: 20,
+// 96 registers with a few spilled, is fastest; 16 holds 128 registers).
+#ifndef LBM_QUAD19_MIN_WARPS
+#define LBM_QUAD19_MIN_WARPS 20
+#endif
+template <int Q>
+constexpr int quad_min_warps() { return Q == 19 ? LBM_QUAD19_MIN_WARPS : kPairMinWarps; }
+
 template <int Q, class S, bool FACES, bool FORCE, int W>
-__global__ void __launch_bounds__(32 * W, kPairMinWarps / W)
+__global__ void __launch_bounds__(32 * W, quad_min_warps<Q>() / W)
     k_step_quad(const __grid_constant__ StepArgs a) {
   using PT = PairT<S>;
   const Geo& g = a.g;
