@@ -284,15 +284,17 @@ void launch_quad_w(const lbm::StepArgs& a, cudaStream_t s) {
 
 // The four-cell form (16-bit storage): rows of a multiple of 128 cells,
 // unpadded state rows, 8-byte aligned planes and a 4-byte aligned wall mask.
-// D3Q19 also takes the four-cell form (a B200 sweep at 256^3: 79.2k MLUPS FP16
-// against 71.7k for pairs, at 20 resident warps and 96 registers).
+// D3Q19 also takes it (a B200 sweep at 256^3: 79.2k MLUPS FP16 against 71.7k
+// for pairs, at 20 resident warps and 96 registers) on rows of a multiple of
+// 256 cells: with one-warp blocks (rows of 128) it keeps 15 warps resident and
+// loses to pairs.
 #ifndef LBM_QUAD_Q19
 #define LBM_QUAD_Q19 1
 #endif
 template <int Q, class S>
 bool quad_ok(const lbm::StepArgs& a) {
-  return (Q == 9 || (LBM_QUAD_Q19 && Q == 19)) && sizeof(S) == 2 && a.g.n2 % 128 == 0 &&
-         a.g.rstride == a.g.n2 &&
+  return (Q == 9 || (LBM_QUAD_Q19 && Q == 19)) && sizeof(S) == 2 &&
+         a.g.n2 % (Q == 19 ? 256 : 128) == 0 && a.g.rstride == a.g.n2 &&
          a.g.pstride % 4 == 0 && reinterpret_cast<uintptr_t>(a.pin) % 8 == 0 &&
          reinterpret_cast<uintptr_t>(a.pout) % 8 == 0 &&
          reinterpret_cast<uintptr_t>(a.wall) % 4 == 0;
