@@ -87,8 +87,10 @@ typedef struct {
                                    the default global gather on B200, kept for
                                    comparison */
 #define LBM_PLAN_SINGLE_CELLS 2u /* rollout steps update one cell per thread
-                                   (the paired two-cell step is otherwise used
-                                   for FP16/BF16 storage when the contiguous
+                                   (FP16/BF16 storage otherwise takes the
+                                   four-cell step on rows of a multiple of 256
+                                   cells for D3Q19 / 128 for D2Q9, else the
+                                   paired two-cell step when the contiguous
                                    extent is even) */
 #define LBM_PLAN_PAIRED_CELLS 4u /* also use the paired two-cell step for FP32
                                    storage (same conditions) */
