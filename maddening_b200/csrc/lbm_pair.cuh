@@ -261,8 +261,9 @@ struct QuadT {
   }
 };
 
-// Resident warps the D3Q19 four-cell budget is set for (sweep 16 / 20 / 24: 20,
-// 96 registers with a few spilled, is fastest; 16 holds 128 registers).
+// Resident warps the D3Q19 four-cell budget is set for (B200 sweep at 256^3,
+// FP16: 16 warps 78.1k, 20 warps 79.4k, 22 / 24 warps 69k MLUPS -- at 20 the 96
+// registers spill a few bytes, beyond it the spills cost more than the warps).
 #ifndef LBM_QUAD19_MIN_WARPS
 #define LBM_QUAD19_MIN_WARPS 20
 #endif
