@@ -270,46 +270,42 @@ struct QuadT {
 template <int Q>
 constexpr int quad_min_warps() { return Q == 19 ? LBM_QUAD19_MIN_WARPS : kPairMinWarps; }
 
-template <int Q, class S, bool FACES, bool FORCE, int W>
-__global__ void __launch_bounds__(32 * W, quad_min_warps<Q>() / W)
-    k_step_quad(const __grid_constant__ StepArgs a) {
+// The populations of quad (k..k+3) of source row `base` pulled along the row:
+// kprev / knext the aligned 32-bit words holding cells k - 1 / k + 4
+// (periodic).
+template <int Q, class S>
+__device__ __forceinline__ void quad_pull(const S* base, int q, uint32_t k, uint32_t kprev,
+                                          uint32_t knext, float (&d)[4][Q]) {
   using PT = PairT<S>;
-  const Geo& g = a.g;
-  const uint32_t row = blockIdx.x;
-  const uint32_t i0 = fdiv(row, g.div_n1);
-  const uint32_t i1 = row - i0 * g.n1;
-  const uint32_t k = blockIdx.y * (128u * W) + 4u * threadIdx.x;
-  const uint32_t kprev = (k == 0 ? g.n2 : k) - 2u;       // word holding cell k - 1 (high)
-  const uint32_t knext = k + 4u == g.n2 ? 0u : k + 4u;  // word holding cell k + 4 (low)
-  const uint32_t i0m = i0 == 0 ? g.n0 - 1 : i0 - 1, i0p = i0 + 1 == g.n0 ? 0u : i0 + 1;
-  const uint32_t i1m = i1 == 0 ? g.n1 - 1 : i1 - 1, i1p = i1 + 1 == g.n1 ? 0u : i1 + 1;
-  const S* pin = static_cast<const S*>(a.pin);
-  float d[4][Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
-    const uint32_t s0 = c0 > 0 ? i0m : (c0 < 0 ? i0p : i0);
-    const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
-    const S* base = pin + (static_cast<uint32_t>(q) * g.pstride + (s0 * g.n1 + s1) * g.rstride);
-    const uint2 v = QuadT<S>::ld(base + k);
-    if (c2 == 0) {
-      d[0][q] = PT::lo(v.x);
-      d[1][q] = PT::hi(v.x);
-      d[2][q] = PT::lo(v.y);
-      d[3][q] = PT::hi(v.y);
-    } else if (c2 > 0) {  // cell j pulls j - 1
-      d[0][q] = PT::hi(PT::ld(base + kprev));
-      d[1][q] = PT::lo(v.x);
-      d[2][q] = PT::hi(v.x);
-      d[3][q] = PT::lo(v.y);
-    } else {  // cell j pulls j + 1
-      d[0][q] = PT::hi(v.x);
-      d[1][q] = PT::lo(v.y);
-      d[2][q] = PT::hi(v.y);
-      d[3][q] = PT::lo(PT::ld(base + knext));
-    }
+  const int c2 = Lat<Q>::c2(q);
+  const uint2 v = QuadT<S>::ld(base + k);
+  if (c2 == 0) {
+    d[0][q] = PT::lo(v.x);
+    d[1][q] = PT::hi(v.x);
+    d[2][q] = PT::lo(v.y);
+    d[3][q] = PT::hi(v.y);
+  } else if (c2 > 0) {  // cell j pulls j - 1
+    d[0][q] = PT::hi(PT::ld(base + kprev));
+    d[1][q] = PT::lo(v.x);
+    d[2][q] = PT::hi(v.x);
+    d[3][q] = PT::lo(v.y);
+  } else {  // cell j pulls j + 1
+    d[0][q] = PT::hi(v.x);
+    d[1][q] = PT::lo(v.y);
+    d[2][q] = PT::hi(v.y);
+    d[3][q] = PT::lo(PT::ld(base + knext));
   }
-  const uint32_t rbase = row * g.n2;
+}
+
+// Everything after the pull of quad (k..k+3) of row (i0, i1): wall swap,
+// faces, moments and collide of each cell, packed stores.  All 32 lanes of the
+// warp call it (vote); `store` = false for lanes that only pad the warp.
+template <int Q, class S, bool FACES, bool FORCE>
+__device__ __forceinline__ void quad_finish(const StepArgs& a, uint32_t i0, uint32_t i1,
+                                            uint32_t k, uint32_t row, float (&d)[4][Q],
+                                            bool store) {
+  const Geo& g = a.g;
+  const uint32_t rbase = row * g.n2, sbase = row * g.rstride;
   bool w[4] = {false, false, false, false};
   if (a.wall != nullptr) {
     const uint32_t w4 = __ldg(reinterpret_cast<const unsigned int*>(a.wall + rbase + k));
@@ -321,6 +317,11 @@ __global__ void __launch_bounds__(32 * W, quad_min_warps<Q>() / W)
     for (int j = 0; j < 4; ++j)
       if (w[j]) wall_swap<Q>(d[j]);
   }
+  Cell x;
+  x.i0 = i0;
+  x.i1 = i1;
+  x.row = rbase;
+  x.srow = sbase;
   if constexpr (FACES) {
     bool near = false;
 #pragma unroll
@@ -336,34 +337,82 @@ __global__ void __launch_bounds__(32 * W, quad_min_warps<Q>() / W)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         if (w[j]) continue;
-        Cell x;
         x.c = rbase + k + j;
-        x.i0 = i0;
-        x.i1 = i1;
         x.k = k + j;
-        x.row = rbase;
-        x.srow = row * g.rstride;
         apply_faces<Q, S>(a, x, d[j]);
       }
     }
   }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    Cell x;
     x.c = rbase + k + j;
-    x.i0 = i0;
-    x.i1 = i1;
     x.k = k + j;
-    x.row = rbase;
-    x.srow = row * g.rstride;
     pair_cell<Q, S, FORCE>(a, x, d[j]);
   }
+  if (!store) return;
   S* pout = static_cast<S*>(a.pout);
-  const uint32_t sbase = row * g.rstride;
 #pragma unroll
   for (int q = 0; q < Q; ++q)
     QuadT<S>::st(pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k), d[0][q], d[1][q],
                  d[2][q], d[3][q]);
+}
+
+// Row-segment form: block = W warps = 128 W consecutive cells of one row.
+template <int Q, class S, bool FACES, bool FORCE, int W>
+__global__ void __launch_bounds__(32 * W, quad_min_warps<Q>() / W)
+    k_step_quad(const __grid_constant__ StepArgs a) {
+  const Geo& g = a.g;
+  const uint32_t row = blockIdx.x;
+  const uint32_t i0 = fdiv(row, g.div_n1);
+  const uint32_t i1 = row - i0 * g.n1;
+  const uint32_t k = blockIdx.y * (128u * W) + 4u * threadIdx.x;
+  const uint32_t kprev = (k == 0 ? g.n2 : k) - 2u;       // word holding cell k - 1 (high)
+  const uint32_t knext = k + 4u == g.n2 ? 0u : k + 4u;  // word holding cell k + 4 (low)
+  const uint32_t i0m = i0 == 0 ? g.n0 - 1 : i0 - 1, i0p = i0 + 1 == g.n0 ? 0u : i0 + 1;
+  const uint32_t i1m = i1 == 0 ? g.n1 - 1 : i1 - 1, i1p = i1 + 1 == g.n1 ? 0u : i1 + 1;
+  const S* pin = static_cast<const S*>(a.pin);
+  float d[4][Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q);
+    const uint32_t s0 = c0 > 0 ? i0m : (c0 < 0 ? i0p : i0);
+    const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
+    quad_pull<Q, S>(pin + (static_cast<uint32_t>(q) * g.pstride + (s0 * g.n1 + s1) * g.rstride),
+                    q, k, kprev, knext, d);
+  }
+  quad_finish<Q, S, FACES, FORCE>(a, i0, i1, k, row, d, true);
+}
+
+// Instance-wide form for any row length that is a multiple of 4: quads follow
+// the linear cell index and each lane finds its own row; the lanes past the
+// last quad redo it without storing.
+template <int Q, class S, bool FACES, bool FORCE>
+__global__ void __launch_bounds__(kBlock, quad_min_warps<Q>() / (kBlock / 32))
+    k_step_gquad(const __grid_constant__ StepArgs a) {
+  const Geo& g = a.g;
+  const uint32_t nquads = g.ncell >> 2;
+  const uint32_t qidx = blockIdx.x * kBlock + threadIdx.x;
+  const bool valid = qidx < nquads;
+  const uint32_t ci = 4u * (valid ? qidx : nquads - 1u);
+  const uint32_t row = fdiv(ci, g.div_n2);
+  const uint32_t k = ci - row * g.n2;
+  const uint32_t i0 = fdiv(row, g.div_n1);
+  const uint32_t i1 = row - i0 * g.n1;
+  const uint32_t kprev = (k == 0 ? g.n2 : k) - 2u;
+  const uint32_t knext = k + 4u == g.n2 ? 0u : k + 4u;
+  const uint32_t i0m = i0 == 0 ? g.n0 - 1 : i0 - 1, i0p = i0 + 1 == g.n0 ? 0u : i0 + 1;
+  const uint32_t i1m = i1 == 0 ? g.n1 - 1 : i1 - 1, i1p = i1 + 1 == g.n1 ? 0u : i1 + 1;
+  const S* pin = static_cast<const S*>(a.pin);
+  float d[4][Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q);
+    const uint32_t s0 = c0 > 0 ? i0m : (c0 < 0 ? i0p : i0);
+    const uint32_t s1 = c1 > 0 ? i1m : (c1 < 0 ? i1p : i1);
+    quad_pull<Q, S>(pin + (static_cast<uint32_t>(q) * g.pstride + (s0 * g.n1 + s1) * g.rstride),
+                    q, k, kprev, knext, d);
+  }
+  quad_finish<Q, S, FACES, FORCE>(a, i0, i1, k, row, d, valid);
 }
 
 // Pairs of the state planes' index: pair j holds state cells 2j, 2j + 1 (rows

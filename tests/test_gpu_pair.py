@@ -4,8 +4,9 @@ the one-cell step for every storage form, lattice, face axis and force mode,
 including the periodic wrap at both ends of a row and every warp/block width
 (contiguous extents 64, 128, 192, 256); the instance-wide pair form for other
 even rows (rows shorter than a warp, pairs whose neighbour lies in the next
-row, a partial last warp); the four-cell form of D2Q9 16-bit storage (rows of
-128, 256, 384, 512 cells); odd rows fall back to the one-cell step."""
+row, a partial last warp); the four-cell form of 16-bit storage (rows of
+128, 256, 384, 512 cells; D2Q9 rows of any multiple of 4); odd rows fall back to
+the one-cell step."""
 
 import numpy as np
 import pytest
@@ -54,6 +55,9 @@ def _node(shape, storage, lattice, kind, cpt, seed=0):
                                            ((1, 1, 64), "D3Q19"), ((40, 128), "D2Q9"),
                                            ((24, 256), "D2Q9"), ((9, 512), "D2Q9"),
                                            ((7, 384), "D2Q9"),
+                                           # instance-wide four-cell form (D2Q9)
+                                           ((31, 36), "D2Q9"), ((5, 100), "D2Q9"),
+                                           ((3, 4), "D2Q9"),
                                            # instance-wide pairs (even rows)
                                            ((3, 4, 100), "D3Q19"), ((5, 3, 34), "D3Q19"),
                                            ((4, 7, 2), "D3Q19"), ((33, 38), "D2Q9"),
