@@ -318,7 +318,7 @@ void launch_gquad(const lbm::StepArgs& a, cudaStream_t s) {
 // multiple of 4 cells (a quad never spans two rows), the same alignment as the
 // row form (4000^2 channel: 148.9k MLUPS against 114.4k for pairs).  D3Q19
 // keeps pairs there: with per-lane rows its 96-register budget spills and it
-// lost (48.3k against 61.9k at 160^3).
+// lost (48.3k against 61.9k at 160^3; 56.4k at 128 registers and 16 warps).
 template <int Q, class S>
 bool gquad_ok(const lbm::StepArgs& a) {
   return Q == 9 && sizeof(S) == 2 && a.g.n2 % 4 == 0 &&
