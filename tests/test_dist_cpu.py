@@ -6,7 +6,6 @@ only rank 0 runs and prints the reference arm."""
 import io
 import os
 import socket
-import sys
 from contextlib import redirect_stdout
 
 import pytest
