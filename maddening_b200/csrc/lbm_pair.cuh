@@ -100,9 +100,10 @@ constexpr int kGPairMinWarps = LBM_GPAIR_MIN_WARPS;
 
 // Moments and collide of one cell whose f_bc populations are in d; `real` =
 // false for the padding cell of a padded row (its result is never read).
+// Returns the cell's stochastic-rounding seed (16-bit storage; else 0).
 template <int Q, class S, bool FORCE>
-__device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, float (&d)[Q],
-                                          bool real = true) {
+__device__ __forceinline__ uint32_t pair_cell(const StepArgs& a, const Cell& x, float (&d)[Q],
+                                              bool real = true) {
   using IO = typename StoreT<S>::IO;
   float F[3] = {0, 0, 0};
   if (FORCE) {
@@ -114,6 +115,8 @@ __device__ __forceinline__ void pair_cell(const StepArgs& a, const Cell& x, floa
   }
   const Mom<float> m = moments<Q, float, FORCE>(d, F);
   collide<Q, float, FORCE>(d, m, F, static_cast<float>(a.omega), static_cast<float>(a.guo_c));
+  if constexpr (sizeof(S) == 2) return sr_seed(x.c, m.u[0], m.u[1], m.u[2], m.rd);
+  else return 0u;
 }
 
 // Everything after the plane loads of one thread's pair (k, k+1) of row
@@ -193,13 +196,19 @@ __device__ __forceinline__ void pair_finish(const StepArgs& a, uint32_t i0, uint
       if (!wb && !last) apply_faces<Q, S>(a, xb, db);  // never on the padding cell
     }
   }
-  pair_cell<Q, S, FORCE>(a, xa, da);
-  pair_cell<Q, S, FORCE>(a, xb, db, !last);
+  const uint32_t sa = pair_cell<Q, S, FORCE>(a, xa, da);
+  const uint32_t sb = pair_cell<Q, S, FORCE>(a, xb, db, !last);
   if (!store) return;
   S* pout = static_cast<S*>(a.pout);
+  const uint32_t s2 = sr_pair(sa, sb);
 #pragma unroll
-  for (int q = 0; q < Q; ++q)
-    PT::st(pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k), da[q], db[q]);
+  for (int q = 0; q < Q; ++q) {
+    S* dst = pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k);
+    if constexpr (sizeof(S) == 2)
+      *reinterpret_cast<uint32_t*>(dst) = sr_two<S>(da[q], db[q], s2);
+    else
+      PT::st(dst, da[q], db[q]);
+  }
 }
 
 // Row-segment form: rows of 64 W cells or a multiple (see the header comment).
@@ -252,12 +261,6 @@ template <class S>
 struct QuadT {
   static __device__ __forceinline__ uint2 ld(const S* p) {
     return __ldg(reinterpret_cast<const uint2*>(p));
-  }
-  static __device__ __forceinline__ void st(S* p, float a, float b, float c, float d) {
-    uint2 w;
-    PairT<S>::st(reinterpret_cast<S*>(&w.x), a, b);
-    PairT<S>::st(reinterpret_cast<S*>(&w.y), c, d);
-    *reinterpret_cast<uint2*>(p) = w;
   }
 };
 
@@ -343,18 +346,23 @@ __device__ __forceinline__ void quad_finish(const StepArgs& a, uint32_t i0, uint
       }
     }
   }
+  uint32_t seed[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     x.c = rbase + k + j;
     x.k = k + j;
-    pair_cell<Q, S, FORCE>(a, x, d[j]);
+    seed[j] = pair_cell<Q, S, FORCE>(a, x, d[j]);
   }
   if (!store) return;
   S* pout = static_cast<S*>(a.pout);
+  const uint32_t s01 = sr_pair(seed[0], seed[1]), s23 = sr_pair(seed[2], seed[3]);
 #pragma unroll
-  for (int q = 0; q < Q; ++q)
-    QuadT<S>::st(pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k), d[0][q], d[1][q],
-                 d[2][q], d[3][q]);
+  for (int q = 0; q < Q; ++q) {
+    uint2 w;
+    w.x = sr_two<S>(d[0][q], d[1][q], s01);
+    w.y = sr_two<S>(d[2][q], d[3][q], s23);
+    *reinterpret_cast<uint2*>(pout + (static_cast<uint32_t>(q) * g.pstride + sbase + k)) = w;
+  }
 }
 
 // Row-segment form: block = W warps = 128 W consecutive cells of one row.
