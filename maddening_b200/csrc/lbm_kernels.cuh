@@ -233,17 +233,16 @@ struct Mom {
 // independent, zero bits truncate).  A value's random bits are the low 16 bits
 // of its own FP32 pattern XOR the cell's hash: uniform whatever the value (the
 // hash is), without a hash per value.
+// Only the low 16 bits of the seed are used: the index and the moments' bits
+// are folded together (rotated apart), one multiply spreads every input bit
+// upwards and the high half is folded back down.
 __device__ __forceinline__ uint32_t sr_seed(uint32_t idx, float u0, float u1, float u2,
                                             float rd) {
-  const uint32_t b1 = __float_as_uint(u1), b2 = __float_as_uint(u2);
-  uint32_t x = idx * 0x9E3779B1u ^ __float_as_uint(u0) ^ __funnelshift_l(b1, b1, 11) ^
-               __funnelshift_l(b2, b2, 22) ^ (__float_as_uint(rd) * 0x27D4EB2Fu);
-  x ^= x >> 15;
-  x *= 0x2C1B3C6Du;
-  x ^= x >> 12;
-  x *= 0x297A2D39u;
-  x ^= x >> 15;
-  return x;
+  const uint32_t b1 = __float_as_uint(u1), b2 = __float_as_uint(u2), b3 = __float_as_uint(rd);
+  uint32_t x = idx ^ __float_as_uint(u0) ^ __funnelshift_l(b1, b1, 11) ^
+               __funnelshift_l(b2, b2, 22) ^ __funnelshift_l(b3, b3, 5);
+  x *= 0x9E3779B1u;
+  return x ^ (x >> 16);
 }
 
 // Random bits of value v of a cell with seed `seed` (the low 16 are used).
