@@ -234,13 +234,12 @@ struct Mom {
 // of its own FP32 pattern XOR the cell's hash: uniform whatever the value (the
 // hash is), without a hash per value.
 // Only the low 16 bits of the seed are used: the index and the moments' bits
-// are folded together (rotated apart), one multiply spreads every input bit
-// upwards and the high half is folded back down.
+// are folded together, one multiply spreads every input bit upwards and the
+// high half is folded back down.
 __device__ __forceinline__ uint32_t sr_seed(uint32_t idx, float u0, float u1, float u2,
                                             float rd) {
-  const uint32_t b1 = __float_as_uint(u1), b2 = __float_as_uint(u2), b3 = __float_as_uint(rd);
-  uint32_t x = idx ^ __float_as_uint(u0) ^ __funnelshift_l(b1, b1, 11) ^
-               __funnelshift_l(b2, b2, 22) ^ __funnelshift_l(b3, b3, 5);
+  uint32_t x = idx ^ __float_as_uint(u0) ^ __float_as_uint(u1) ^ __float_as_uint(u2) ^
+               __float_as_uint(rd);
   x *= 0x9E3779B1u;
   return x ^ (x >> 16);
 }
