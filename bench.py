@@ -770,7 +770,7 @@ def main():
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
     ap.add_argument("--c5-steps", type=int, default=2000,
                     help="steps of the 512^3 precision comparison (variants)")
-    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9", "c1"],
+    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9", "c1", "batched"],
                     help="run one variant alone and print its JSON (for profiling)")
     ap.add_argument("--variant-grid", default=None,
                     help="lattice of --only, e.g. 192x128x128 (default: the variant's own)")
@@ -783,10 +783,10 @@ def main():
         import torch
         dev = torch.device("cuda", 0)
         kw = {}
-        if args.variant_grid:
+        if args.variant_grid and args.only != "batched":
             kw["grid"] = tuple(int(v) for v in args.variant_grid.split("x"))
         fn = {"pipe": pipe_cost, "update_call": update_call_cost, "frames": frames_cost,
-              "d2q9": d2q9_cost, "c1": c1_cost}[args.only]
+              "d2q9": d2q9_cost, "c1": c1_cost, "batched": batched_cost}[args.only]
         if args.only == "pipe":
             kw["steps"] = args.steps
         print(json.dumps({args.only: fn(dev, **kw)}), flush=True)
