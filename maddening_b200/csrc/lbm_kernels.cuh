@@ -374,11 +374,13 @@ __device__ __forceinline__ void collide(R (&d)[Q], const Mom<R>& m, const R (&F)
     const R eu = dot_e(e0, e1, e2, m.u);
     const R dq = d[q], dop = d[o];
     if constexpr (FORCE) {
-      R A = fma_r(r45, mul_r(eu, eu), base);
-      R B = mul_r(r3, eu);
+      // c 9 e.F and c 3 e.F depend on the force only: the cells of a thread
+      // that share a uniform force share them
       const R eF = dot_e(e0, e1, e2, F);
-      A = add_r(A, fma_r(mul_r(c9, eu), eF, -cuF));
-      B = fma_r(c3, eF, B);
+      const R c9eF = mul_r(c9, eF), c3eF = mul_r(c3, eF);
+      R A = fma_r(r45, mul_r(eu, eu), base);
+      A = add_r(A, fma_r(eu, c9eF, -cuF));
+      const R B = fma_r(r3, eu, c3eF);
       d[q] = add_r(fma_r(keep, dq, A), B);
       d[o] = sub_r(fma_r(keep, dop, A), B);
     } else {
