@@ -325,11 +325,11 @@ def run_ours(args):
         torch.cuda.empty_cache()
 
     if not args.no_variants and rank == 0:
-        variants["precision_512"] = precision_cost(dev, args.c5_steps)
+        # shorter measurements first; the 512^3 precision study (tens of seconds
+        # at the power cap) last, so that its heat does not slow the others
+        variants["batched"] = batched_cost(dev)
         torch.cuda.empty_cache()
         variants["adjoint"] = adjoint_cost(dev)
-        torch.cuda.empty_cache()
-        variants["batched"] = batched_cost(dev)
         torch.cuda.empty_cache()
         variants["pipe"] = pipe_cost(dev)
         torch.cuda.empty_cache()
@@ -340,6 +340,8 @@ def run_ours(args):
         variants["update_call"] = update_call_cost(dev)
         torch.cuda.empty_cache()
         variants["frames"] = frames_cost(dev)
+        torch.cuda.empty_cache()
+        variants["precision_512"] = precision_cost(dev, args.c5_steps)
 
     if rank == 0:
         peak, peak_kind = _peaks()
