@@ -19,9 +19,11 @@
 // outputs) and collides again, writing p for the next step: 19 loads and 19
 // stores per cell, each warp access one contiguous 32-element run.
 //
-// One thread owns one cell.  On B200 this beat 2- and 4-cell vector forms:
-// the wider forms need more registers than 32 resident warps per SM allow,
-// and the lost occupancy costs more than the wider accesses save.
+// One thread owns one cell.  For FP32 storage this beat 2- and 4-cell vector
+// forms on B200: the wider forms need more registers than 32 resident warps
+// per SM allow, and the lost occupancy costs more than the wider accesses save.
+// 16-bit storage moves too few bytes per cell for that: it takes two or four
+// cells per thread (lbm_pair.cuh) and rounds stochastically (below).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -60,12 +62,7 @@ template <>
 __device__ __forceinline__ float from_r<float>(float v) { return v; }
 template <>
 __device__ __forceinline__ double from_r<double>(double v) { return v; }
-template <>
-__device__ __forceinline__ __half from_r<__half>(float v) { return __float2half_rn(v); }
-template <>
-__device__ __forceinline__ __nv_bfloat16 from_r<__nv_bfloat16>(float v) {
-  return __float2bfloat16_rn(v);
-}
+// 16-bit storage rounds stochastically (sr_one / sr_two below).
 
 template <class S>
 __device__ __forceinline__ typename StoreT<S>::R ld_pop(const S* p) {

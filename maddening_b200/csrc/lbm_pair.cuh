@@ -53,10 +53,6 @@ struct PairT<__half> {
   static __device__ __forceinline__ float hi(P v) {
     return __high2float(*reinterpret_cast<const __half2*>(&v));
   }
-  static __device__ __forceinline__ void st(__half* p, float a, float b) {
-    const __half2 h = __floats2half2_rn(a, b);
-    *reinterpret_cast<unsigned int*>(p) = *reinterpret_cast<const unsigned int*>(&h);
-  }
 };
 
 template <>
@@ -67,10 +63,6 @@ struct PairT<__nv_bfloat16> {
   }
   static __device__ __forceinline__ float lo(P v) { return __uint_as_float(v << 16); }
   static __device__ __forceinline__ float hi(P v) { return __uint_as_float(v & 0xffff0000u); }
-  static __device__ __forceinline__ void st(__nv_bfloat16* p, float a, float b) {
-    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-    *reinterpret_cast<unsigned int*>(p) = *reinterpret_cast<const unsigned int*>(&h);
-  }
 };
 
 template <>
