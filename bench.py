@@ -319,6 +319,7 @@ def run_ours(args):
             tv = a0.elapsed_time(a1) / 1e3
             mv = cells * K / tv / 1e6
             variants[storage] = {"mlups": round(mv, 1), "steps": K, "bytes_per_cell": 76,
+                                 "rounding": "stochastic (cvt.rs)",
                                  "over_fp32": round(mv / (mlups / world), 3),
                                  "hbm_frac": round(mv * 1e6 * 76 / 1e9 / _peaks()[0], 4)}
             del vn, vs
