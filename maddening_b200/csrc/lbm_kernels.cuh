@@ -902,7 +902,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks<S>())
 // A tile is kBatchTile consecutive cells of one instance (a multiple of
 // 2 kBlock: the paired kernel gives each thread kBatchTile / (2 kBlock) pairs).
 // 512 cells: on the 64-lattice ensemble 37.4k (FP32) and 54.8k (FP16) MLUPS
-// against 36.7k / 52.6k for 256-cell tiles (B200).
+// against 36.7k / 52.6k for 256-cell tiles, 36.6k / 55.0k for 1024 and
+// 36.0k / 53.1k for 2048 (B200).
 #ifndef LBM_BATCH_TILE
 #define LBM_BATCH_TILE (4 * LBM_STEP_BLOCK)
 #endif
