@@ -62,3 +62,28 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     with redirect_stdout(buf):
         bench.run_reference(type("A", (), {"warmup": 3, "steps": 2})())
     assert buf.getvalue() == ""
+
+
+def test_reference_arm_line_on_rank_zero(monkeypatch):
+    """Rank 0 prints one JSON line for the CPU port: bounded warm-up (>= 3) and
+    timed steps, the measured value repeated as cpu_baseline and e2e."""
+    import json
+    calls = []
+
+    def fake_cpu_baseline(procs, nx, steps):
+        calls.append(steps)
+        return 3.5, 1.0
+
+    monkeypatch.setenv("WORLD_SIZE", "1")
+    monkeypatch.setenv("RANK", "0")
+    monkeypatch.setattr(bench, "cpu_baseline", fake_cpu_baseline)
+    monkeypatch.setattr(bench, "_host_cores", lambda: 4)
+    buf = io.StringIO()
+    with redirect_stdout(buf):
+        bench.run_reference(type("A", (), {"warmup": 10, "steps": 1000})())
+    line = json.loads(buf.getvalue())
+    assert calls == [3, 8]
+    assert line["impl"] == "reference" and line["warmup"] == 3 and line["steps"] == 8
+    assert line["value"] == line["cpu_baseline"]["value"] == line["e2e"]["value"] == 3.5
+    assert line["cpu_baseline"]["cores"] == 4 and line["cpu_baseline"]["kind"] == "port"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
