@@ -29,6 +29,7 @@ nothing at test time reads the reference.
 from __future__ import annotations
 
 import importlib
+import os
 import sys
 import types
 from pathlib import Path
@@ -537,7 +538,10 @@ def unit_vectors(lbm, jnp, seed=7):
     return out
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
+    ref_root = ref_root or os.environ.get("MADDENING_REF_ROOT")
+    if not ref_root:
+        sys.exit("usage: make_golden.py <reference root> (or set MADDENING_REF_ROOT)")
     ref_root = Path(ref_root)
     lbm = _install_shims(ref_root)
     jnp = sys.modules["jax.numpy"]
