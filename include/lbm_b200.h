@@ -94,6 +94,16 @@ typedef struct {
                                    extent is even) */
 #define LBM_PLAN_PAIRED_CELLS 4u /* also use the paired two-cell step for FP32
                                    storage (same conditions) */
+#define LBM_PLAN_TWO_PASS 8u /* lbm_update and the first step of lbm_rollout run
+                                as two passes (collide into the workspace, then
+                                the pull step) instead of the one-pass tiled
+                                kernel; same results bit for bit */
+#define LBM_PLAN_TEST_WAIT_TIMEOUT 16u /* test hook: the one-pass tiled kernel arms
+                                its barriers but issues no copies and gives up a
+                                wait after 0.2 ms (instead of 2 s), so its waits
+                                run out: it sets the status word and returns
+                                early with the outputs incomplete.  Only for
+                                testing the timeout path */
 
 typedef struct {
   int32_t lattice;  /* lbm_lattice: 19 (D3Q19) or 9 (D2Q9)                */

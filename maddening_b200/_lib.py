@@ -38,6 +38,8 @@ class LbmError(RuntimeError):
 PLAN_STAGED_ROWS = 1
 PLAN_SINGLE_CELLS = 2
 PLAN_PAIRED_CELLS = 4
+PLAN_TWO_PASS = 8
+PLAN_TEST_WAIT_TIMEOUT = 16
 
 
 class lbm_desc(C.Structure):

@@ -19,18 +19,7 @@
 #include "lbm_pack.cuh"
 #include "lbm_pipe.cuh"
 #include "lbm_staged.cuh"
-
-struct lbm_plan {
-  int Q = 0, D = 0, storage = 0;
-  int64_t shape[3] = {0, 0, 0};  // reference grid_shape
-  lbm::Geo g{};                  // internal geometry
-  double tau = 0;
-  size_t elem = 4;               // bytes per stored population
-  size_t io = 4;                 // bytes per f / force / moment element
-  uint32_t flags = 0;            // LBM_PLAN_* bits
-};
-
-namespace {
+#include "lbm_host.h"
 
 thread_local std::string g_last_error;
 
@@ -48,6 +37,8 @@ int cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   return LBM_OK;
 }
+
+namespace {
 
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
@@ -414,6 +405,30 @@ int launch_step_moments_only(const lbm::StepArgs& a, cudaStream_t s) {
   return cuda_check(cudaGetLastError(), "k_step launch");
 }
 
+// One-pass tiled step (lbm_tiled.cuh) for lbm_update and the first step of a
+// rollout: 32-bit IO, rows of a multiple of 4 cells (16-byte copy groups),
+// 16-byte aligned reference-layout buffers that do not overlap, an unpadded
+// whole lattice.
+template <class S>
+bool tiled_ok(const lbm_plan* p, const lbm::StepArgs& a, const void* ws, bool aos_out) {
+  if constexpr (sizeof(typename lbm::StoreT<S>::IO) != 4) {
+    return false;
+  } else {
+    if (p->flags & LBM_PLAN_TWO_PASS) return false;
+    if (p->g.n2 % 4 != 0 || p->g.rstride != p->g.n2 || a.face_inset != 0 || a.force_mode == 3)
+      return false;
+    const uintptr_t fi = reinterpret_cast<uintptr_t>(a.f_in);
+    const uintptr_t fo = reinterpret_cast<uintptr_t>(a.f_out);
+    if (fi % 16 != 0) return false;
+    if (aos_out) {
+      // f_out is written while other blocks still read f_in: no overlap
+      const uintptr_t bytes = static_cast<uintptr_t>(p->g.ncell) * p->Q * 4;
+      if (fo % 16 != 0 || (fo < fi + bytes && fi < fo + bytes)) return false;
+    }
+    return reinterpret_cast<uintptr_t>(ws) % 4 == 0;  // the status word
+  }
+}
+
 // Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies
 // (with n > 1 also the status word after them).
 template <int Q, class S>
@@ -423,18 +438,37 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   char* A = ws;
   char* B = ws + sb;
   a.f_in = f_in;
+  a.f_out = f_out;
+  int rc;
+  if constexpr (sizeof(typename lbm::StoreT<S>::IO) == 4) {
+    if (n == 1 && tiled_ok<S>(p, a, ws, true)) {
+      // the whole update in one pass; the workspace holds only the status word
+      a.status = reinterpret_cast<int*>(ws);
+      rc = cuda_check(cudaMemsetAsync(a.status, 0, sizeof(int), s), "cudaMemsetAsync");
+      if (rc) return rc;
+      return launch_tiled<Q, S, lbm::kOutAoS>(p, a, s);
+    }
+  }
   a.pout = A;
   lbm::StepArgs m = a;  // the first pass and intermediate steps write no moments
   m.rho = m.vel = m.prs = nullptr;
-  int rc = launch_prepare<Q, S>(m, s);
-  if (rc) return rc;
   // The bulk copies need 16-byte aligned rows: the caller's workspace too.
   const bool staged = n > 1 && staged_ok<Q, S>(p) && reinterpret_cast<uintptr_t>(ws) % 16 == 0;
-  if (staged) {
+  const bool tiled = n > 1 && tiled_ok<S>(p, a, ws + 2 * sb, false);
+  if (staged || tiled) {
     m.status = reinterpret_cast<int*>(ws + 2 * sb);
     rc = cuda_check(cudaMemsetAsync(m.status, 0, sizeof(int), s), "cudaMemsetAsync");
     if (rc) return rc;
   }
+  if (tiled) {
+    // step 1 straight from the reference layout (p after one step into A)
+    if constexpr (sizeof(typename lbm::StoreT<S>::IO) == 4)
+      rc = launch_tiled<Q, S, lbm::kOutState>(p, m, s);
+    --n;
+  } else {
+    rc = launch_prepare<Q, S>(m, s);
+  }
+  if (rc) return rc;
   for (int64_t i = 0; i + 1 < n; ++i) {
     m.pin = A;
     m.pout = B;

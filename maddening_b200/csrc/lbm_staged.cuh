@@ -79,6 +79,26 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return false;
 }
 
+// This CTA's shared memory -> global, `bytes` a multiple of 16, both addresses
+// 16-byte aligned; tracked in the issuing thread's bulk async-group, which
+// this call commits.
+__device__ __forceinline__ void bulk_store_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// The issuing thread's bulk stores have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read_all() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// The issuing thread's bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // 1024 resident threads per SM (<= 64 registers) for 32-bit arithmetic, 512
 // for FP64.
 template <class S, int T>
