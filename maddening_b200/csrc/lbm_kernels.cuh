@@ -661,11 +661,14 @@ __device__ __forceinline__ void store_moments(const StepArgs& a, uint32_t c,
   }
 }
 
-// Reference state f (IO) -> normalised offset, and back.
+// Reference state f (IO) -> normalised offset, and back.  The offset
+// d = (f - w_q) / w_q = f (1 / w_q) - 1 is one fused multiply-add: 1 / w_q is
+// an integer or a short binary fraction (D3Q19: 3, 18, 36; D2Q9: 2.25, 9,
+// 36), exact in float and double, so the FMA forms f / w_q - 1 exactly and
+// rounds it once.
 template <int Q, class R>
 __device__ __forceinline__ R to_offset(R f, int q) {
-  if constexpr (sizeof(R) == 8) return mul_r(sub_r(f, Lat<Q>::w(q)), 1.0 / Lat<Q>::w(q));
-  else return mul_r(sub_r(sub_r(f, w_hi<Q>(q)), w_lo<Q>(q)), static_cast<float>(1.0 / Lat<Q>::w(q)));
+  return fma_r(f, static_cast<R>(static_cast<double>(Lat<Q>::kWDen) / Lat<Q>::wr(q)), R(-1));
 }
 template <int Q, class R>
 __device__ __forceinline__ R from_offset(R d, int q) {

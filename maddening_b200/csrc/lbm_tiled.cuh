@@ -56,7 +56,8 @@ template <>
 struct Sweep<19> {
   static constexpr int TY = 8, TZ = 32;  // tile rows (a1) x row cells (a2)
   static constexpr int HR = 1;           // halo rows
-  static constexpr int NCW = 11;         // collide warps: (8 + 2) x (32 + 2) = 340 cells
+  static constexpr int NCW = 6;          // collide warps, two cells per lane:
+  static constexpr int CPL = 2;          //   (8 + 2) x (32 + 2) = 340 <= 6 x 32 x 2
   static constexpr int MINB = 1;         // resident blocks per SM
   __host__ __device__ static constexpr int cs(int q) { return Lat<19>::c0(q); }  // sweep
   __host__ __device__ static constexpr int cr(int q) { return Lat<19>::c1(q); }  // rows
@@ -65,7 +66,8 @@ template <>
 struct Sweep<9> {
   static constexpr int TY = 1, TZ = 128;
   static constexpr int HR = 0;
-  static constexpr int NCW = 5;  // 130 cells
+  static constexpr int NCW = 3;  // 130 cells <= 3 x 32 x 2
+  static constexpr int CPL = 2;
   static constexpr int MINB = 2;
   __host__ __device__ static constexpr int cs(int q) { return Lat<9>::c1(q); }
   __host__ __device__ static constexpr int cr(int) { return 0; }
@@ -82,10 +84,11 @@ struct TileShape {
   static constexpr int CW = TZ + 2;                   // collided cells per row
   static constexpr int PLANE = RP * W * Q;            // IO elements per plane slot
   static constexpr int NCW = Sweep<Q>::NCW;           // collide warps
+  static constexpr int CPL = Sweep<Q>::CPL;           // cells per collide lane
   static constexpr int NOW = TY * TZ / 32;            // output warps (32 cells each)
   static constexpr int NT = 32 * (1 + NCW + NOW);     // + the producer warp
   static_assert(TZ % 32 == 0, "an output warp covers 32 cells of one tile row");
-  static_assert(32 * NCW >= RP * CW, "one collided cell per collide lane and plane");
+  static_assert(32 * NCW * CPL >= RP * CW, "CPL collided cells per collide lane and plane");
 };
 
 // Barriers and flags of a block, after the slots and the staging rows.
@@ -301,15 +304,19 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t pari
 
 // Wait bounded by wall time (limit_ns of the global timer) that also ends when
 // another warp of the block has given up (*abort set); a wait that runs out
-// sets *abort itself.
+// sets *abort itself.  Between polls the warp sleeps, up to max_sleep_ns, so
+// that waiting warps leave the issue slots to the working ones.
 __device__ __forceinline__ bool tile_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns,
-                                          volatile int* abort) {
+                                          volatile int* abort, uint32_t max_sleep_ns) {
   if (mbar_try_wait_sleep(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
+  uint32_t sleep = 32;
   for (;;) {
     if (mbar_try_wait_sleep(bar, parity)) return true;
     if (*abort) return false;
     if (globaltimer_ns() - t0 > limit_ns) break;
+    __nanosleep(sleep);
+    sleep = sleep < max_sleep_ns ? 2 * sleep : max_sleep_ns;
   }
   *abort = 1;
   return false;
@@ -353,7 +360,8 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
       uint32_t P = 0;
       for (; L.item < t.items; plane_next<Q>(a, t, L), ++P) {
         const uint32_t sl = P % S_;
-        if (P >= S_ && !tile_wait(&sync->consumed[sl], (P / S_ - 1) & 1u, t.wait_ns, abort))
+        if (P >= S_ &&
+            !tile_wait(&sync->consumed[sl], (P / S_ - 1) & 1u, t.wait_ns, abort, 1024))
           break;
         fence_proxy_async_smem();
         tiled_issue<Q>(a, t, L, planes + static_cast<size_t>(sl) * T::PLANE, &sync->full[sl]);
@@ -361,34 +369,54 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
       sync->issued = P;
     }
   } else if (warp <= static_cast<uint32_t>(T::NCW)) {
-    // ---- collide warps: plane P in place once it has landed
-    const uint32_t m = (warp - 1) * 32 + lane;  // this lane's cell of the plane
-    const uint32_t rr = m / T::CW, cc = m % T::CW;
-    const uint32_t soff = (rr * T::W + kTileHalo - 1 + cc) * Q;  // its place in a slot
+    // ---- collide warps: plane P in place once it has landed; lane cells
+    // m_k = lane + 32 (warp - 1 + k NCW), k < CPL, their loads issued together
+    using T2 = TileShape<Q>;
+    uint32_t soff[T2::CPL], rr[T2::CPL], cc[T2::CPL], rz[T2::CPL];
+    bool mine[T2::CPL];
+#pragma unroll
+    for (int k = 0; k < T2::CPL; ++k) {
+      const uint32_t m = (warp - 1 + k * T2::NCW) * 32 + lane;
+      rr[k] = m / T::CW;
+      cc[k] = m % T::CW;
+      soff[k] = (rr[k] * T::W + kTileHalo - 1 + cc[k]) * Q;  // its place in a slot
+      mine[k] = false;
+      rz[k] = 0;
+    }
     PlaneRef C;
     plane_first<Q>(a, t, blockIdx.x, C);
-    uint32_t P = 0, item = ~0u, rz = 0;
-    bool mine = false;
+    uint32_t P = 0, item = ~0u;
     for (; C.item < t.items; plane_next<Q>(a, t, C), ++P) {
-      if (C.item != item) {  // a new work item: this lane's row and column
+      if (C.item != item) {  // a new work item: the lane cells' rows and columns
         item = C.item;
-        mine = rr < C.tyv + 2 * T::HR && cc < C.tzv + 2;
-        rz = wrapu(static_cast<int>(C.y0 + rr) - T::HR, t.NR) * t.SR +
-             wrapu(static_cast<int>(C.z0 + cc) - 1, g.n2);
+#pragma unroll
+        for (int k = 0; k < T2::CPL; ++k) {
+          mine[k] = rr[k] < C.tyv + 2 * T::HR && cc[k] < C.tzv + 2;
+          rz[k] = wrapu(static_cast<int>(C.y0 + rr[k]) - T::HR, t.NR) * t.SR +
+                  wrapu(static_cast<int>(C.z0 + cc[k]) - 1, g.n2);
+        }
       }
       const uint32_t sl = P % S_;
-      const bool ok = tile_wait(&sync->full[sl], (P / S_) & 1u, t.wait_ns, abort);
+      const bool ok = tile_wait(&sync->full[sl], (P / S_) & 1u, t.wait_ns, abort, 1024);
       if (!__all_sync(0xffffffffu, ok)) break;
       if (lane == 0) atomicMax(&sync->landed, P + 1);
-      if (mine) {
-        const uint32_t c = plane_s(t, C) * t.SS + rz;
-        float* cell = planes + static_cast<size_t>(sl) * T::PLANE + soff;
-        R d[Q];
+      float* slot = planes + static_cast<size_t>(sl) * T::PLANE;
+      const uint32_t cs0 = plane_s(t, C) * t.SS;
+      R d[T2::CPL][Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) d[q] = to_offset<Q, R>(cell[q], q);
-        collide_ref<Q, S, FORCE>(a, c, d);
+      for (int k = 0; k < T2::CPL; ++k) {
+        if (mine[k]) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) cell[q] = d[q];
+          for (int q = 0; q < Q; ++q) d[k][q] = to_offset<Q, R>(slot[soff[k] + q], q);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < T2::CPL; ++k) {
+        if (mine[k]) {
+          collide_ref<Q, S, FORCE>(a, cs0 + rz[k], d[k]);
+#pragma unroll
+          for (int q = 0; q < Q; ++q) slot[soff[k] + q] = d[k][q];
+        }
       }
       fence_proxy_async_smem();  // before the slot is refilled by a copy
       __syncwarp();
@@ -408,7 +436,8 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
     for (; O.item < t.items; plane_next<Q>(a, t, O), ++P) {
       if (O.j < 1 || O.j > O.nv) continue;
       const uint32_t sn = (P + 1) % S_;
-      const bool ok = tile_wait(&sync->collided[sn], ((P + 1) / S_) & 1u, t.wait_ns, abort);
+      const bool ok =
+          tile_wait(&sync->collided[sn], ((P + 1) / S_) & 1u, t.wait_ns, abort, 64);
       if (!__all_sync(0xffffffffu, ok)) break;
       const uint32_t ps = plane_s(t, O);
       const bool act = ty < O.tyv && tz < O.tzv;
@@ -511,7 +540,7 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
     // copies issued and not seen landing: wait for them (bounded) before exit
     sync->abort = 0;
     for (uint32_t P = sync->landed; P < sync->issued; ++P)
-      if (!tile_wait(&sync->full[P % S_], (P / S_) & 1u, t.wait_ns, abort)) break;
+      if (!tile_wait(&sync->full[P % S_], (P / S_) & 1u, t.wait_ns, abort, 512)) break;
   }
 }
 
