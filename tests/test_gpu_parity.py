@@ -5,6 +5,9 @@
   fused ``run`` (offsets kept on the device), FP32 and FP64 storage;
 * the 64^3 force-driven channel, 500 steps, FP32 vs the FP64 oracle: relative
   L2 of density and velocity <= 1e-5 (the north-star bound);
+* the benchmark's obstacle flow (seeded spheres, velocity inlet 0.05,
+  zero-gradient outlet) at 64^3, 500 steps: FP32 <= 1e-5 and FP16 storage
+  <= 1e-3 against the FP64 oracle's run (tests/golden/obstacle64.npz);
 * the documented face extensions against the oracle.
 
 Tolerances are written per test.
@@ -121,6 +124,40 @@ def test_channel64_500_steps_fp32_within_1e5_of_fp64(golden):
           f"(rho-1)={float(ref['f32_relL2_rho_dev']):.2e}")
     assert e_rho <= 1e-5
     assert e_u <= 1e-5
+
+
+@pytest.mark.parametrize("storage,tol", [("f32", 1e-5), ("f16", 1e-3)])
+def test_obstacle64_500_steps_vs_fp64_oracle(storage, tol):
+    """The benchmark workload's physics at 64^3: seeded sphere obstacles (radii
+    4-12, 10 % solid), velocity inlet u = (0.05, 0, 0) at x_min, zero-gradient
+    outlet at x_max, periodic y/z, tau 0.6, from rest; 500 steps against the
+    FP64 oracle (tests/golden/make_obstacle64.py).  Bounds: FP32 storage 1e-5
+    relative L2 on density and velocity, FP16 storage 1e-3 (also on rho - 1).
+    The inlet and outlet are extensions: parity is against the oracle's
+    restatement of them, not the reference (which has neither)."""
+    from maddening_b200 import LBMNode
+    from maddening_b200.geometry import random_spheres
+    import os
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "obstacle64.npz"))
+    grid = (64, 64, 64)
+    wall = random_spheres(grid, seed=0)
+    np.testing.assert_array_equal(np.packbits(wall.reshape(-1)), ref["wall_bits"])
+    node = LBMNode("obst64", 1.0, grid_shape=grid, viscosity=0.1 / 3.0, wall_mask=wall,
+                   outlet_condition="zero_gradient", storage=storage)
+    out = node.run(node.initial_state(), {"inlet_velocity": np.array([0.05, 0.0, 0.0])}, 500)
+    rho = out["density"].cpu().numpy().astype(np.float64)
+    u = out["velocity"].cpu().numpy()
+    rd_ref = ref["x64_rho_dev"].astype(np.float64)
+    e_rho = R.rel_l2(rho, 1.0 + rd_ref)
+    e_rd = R.rel_l2(rho - 1.0, rd_ref)
+    e_u = R.rel_l2(u, ref["x64_u"])
+    print(f"\nobstacle64 {storage} vs FP64 oracle: relL2 rho={e_rho:.2e} u={e_u:.2e} "
+          f"(rho-1)={e_rd:.2e}; the reference's float32 arithmetic: rho="
+          f"{float(ref['f32_relL2_rho']):.2e} u={float(ref['f32_relL2_u']):.2e}")
+    assert e_rho <= tol
+    assert e_u <= tol
+    if storage == "f16":
+        assert e_rd <= tol
 
 
 def _small_obstacle_case(lattice="D3Q19", grid=(16, 8, 12), seed=3):
