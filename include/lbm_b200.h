@@ -327,9 +327,11 @@ int lbm_batch_rollout(const lbm_batch* batch, lbm_stream_t stream, const void* c
  * scratch is a static device array of LBM_NOALLOC_SCRATCH_BYTES inside the
  * library, which every GPU that loads the library holds until the process
  * exits.  It allocates nothing (no cudaMalloc / cudaFree / allocating library
- * call).  Its first call on a device looks up that array's device address with
- * the device current, so make the first call on each device before any stream
- * capture.  Lattices whose populations need more than the array are rejected
+ * call).  Every call looks up that array's device address in the current
+ * context and keeps none between calls, so a device reset or another context
+ * on the same device never leaves it a stale address; the first lookup on a
+ * device also loads the library's code there, so make the first call on each
+ * device before any stream capture.  Lattices whose populations need more than the array are rejected
  * with LBM_ERR_WORKSPACE.  All calls share the one array: calls that overlap on
  * the GPU (different streams, or different threads without ordering) race and
  * corrupt each other; order them on one stream.  The array keeps the last

@@ -7,7 +7,6 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -889,30 +888,20 @@ struct lbm_batch {
 // Scratch of lbm_update_noalloc: one population copy, in the module's static
 // device memory (every GPU that loads the library holds it until exit).  In
 // host code this name is a host-side stand-in, not a device address; the
-// device address comes from cudaGetSymbolAddress, once per device.
+// device address comes from cudaGetSymbolAddress with the device current.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[LBM_NOALLOC_SCRATCH_BYTES];
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device; looked up on the
-// first call per device (that device current), then cached.
+// Device address of g_noalloc_scratch in the current context, looked up on
+// every call (cheap once the module is loaded there): an address kept from
+// an earlier call could belong to a context that has since been reset or
+// replaced.  The first lookup on a device loads the library's module there.
 int noalloc_scratch(void** out) {
-  int dev = 0;
-  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  void* p = nullptr;
+  const int rc = cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
   if (rc) return rc;
-  if (dev < 0 || dev >= kMaxDevices) return fail(LBM_ERR_UNSUPPORTED, "device %d", dev);
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (g_noalloc_ptr[dev] == nullptr) {
-    void* p = nullptr;
-    rc = cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-    if (rc) return rc;
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
+  *out = p;
   return LBM_OK;
 }
 
