@@ -16,9 +16,15 @@ A "step" is one lattice update of all 16.8 M cells; the metric is MLUPS
   rollout, device->host copy of f, density, velocity and pressure, all inside
   the timed region (bytes reported per lattice step).
 * ``roofline``: 152 algorithmic bytes per cell-update (19 loads + 19 stores of
-  4 B) over the measured HBM copy bandwidth.
+  4 B) of the state-step kernel over its average launch time, measured with
+  CUDA events as (t(K steps) - t(2 steps)) / (K - 2), against the measured
+  HBM copy bandwidth.
+* ``update_call``: one ``LBMNode.update`` per step (the call a graph manager
+  makes), reference-layout state in and out of every call.
+* ``clocks``: SM clock and throttle reasons sampled through NVML every 2 ms
+  from the warm-up to the end of the timed region.
 * ``cpu_baseline``: the CPU restatement of the reference step (the oracle) on
-  a bounded sample of the same workload, on this host's cores.
+  a bounded sample of the same workload, one process per host core.
 * ``--impl reference``: the reference's CPU implementation of the path.  JAX
   (the reference's array runtime) is not installed on this image, so the
   restatement of the reference step stands in for it, on all host cores.
@@ -34,9 +40,10 @@ import ctypes as C
 import json
 import multiprocessing as mp
 import os
+import platform
 import statistics
-import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -126,52 +133,99 @@ def _host_cores():
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, power and throttle reasons of one GPU, read through NVML (read
+    only) by a thread every ``period`` seconds while the context is open."""
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown",
+               0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
+
+    def __init__(self, torch_device, period: float = 0.002):
+        self.period = period
+        self.rows = []
+        self.err = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            try:
+                props = torch.cuda.get_device_properties(torch_device)
+                bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id,
+                                            props.pci_device_id)
+                self._h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:  # noqa: BLE001
+                self._h = pynvml.nvmlDeviceGetHandleByIndex(torch.device(torch_device).index or 0)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+        except Exception as e:  # noqa: BLE001
+            self.err = f"NVML unavailable: {e}"
+
+    def _sample(self):
+        nv = self._nv
+        try:
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        except AttributeError:
+            reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self._h)
+        self.rows.append((time.perf_counter(),
+                          float(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)),
+                          nv.nvmlDeviceGetPowerUsage(self._h) / 1000.0, int(reasons)))
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception as e:  # noqa: BLE001
+                self.err = str(e)
+                return
+            self._stop.wait(self.period)
 
     def __enter__(self):
-        try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.fh, stderr=subprocess.DEVNULL)
-        except Exception:  # noqa: BLE001
-            self.proc = None
+        if self._h is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            self.proc.wait(timeout=10)
-            self.fh.close()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
-    def summary(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
-        with open(self.path) as fh:
+    def summary(self, t0=None, t1=None):
+        """Median SM clock and the reasons seen; with t0/t1 (perf_counter
+        seconds) also the samples taken inside that window."""
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "no samples"]}
+        sm = [r[1] for r in self.rows]
+        loaded = [x for x in sm if x > 0.5 * max(sm)]
+        reasons = sorted({name for r in self.rows for bit, name in self.REASONS.items()
+                          if r[3] & bit})
+        out = {"sm_mhz": statistics.median(loaded), "sm_max_mhz": self.max_mhz,
+               "reasons": reasons, "samples": len(self.rows), "source": "NVML",
+               "power_w_max": round(max(r[2] for r in self.rows), 1)}
+        if t0 is not None:
+            inside = [r[1] for r in self.rows if t0 <= r[0] <= t1]
+            out["samples_in_timed_region"] = len(inside)
+            if inside:
+                out["sm_mhz_timed_region"] = statistics.median(inside)
+        return out
+
+
+def host_info():
+    model = platform.processor() or "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
             for line in fh:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
-        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
-        return {"sm_mhz": statistics.median(loaded) if loaded else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "cpu_count": os.cpu_count(), "affinity": _host_cores(),
+            "reference_runtime": "reference JAX CPU path unavailable on this box (jax is not "
+                                 "installed and has no offline wheel); the float32 "
+                                 "restatement of the reference step stands in"}
 
 
 # ---------------------------------------------------------------------------
@@ -257,21 +311,36 @@ def run_ours(args):
                                    dst.data_ptr(), int(n), C.byref(sargs), C.byref(mom),
                                    ws.data_ptr(), ws.numel()))
 
-    rollout(f_a, f_b, max(args.warmup, 3))
-    _barrier(world)
     K = args.steps
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(dev) as clk:
+        rollout(f_a, f_b, max(args.warmup, 3))
         _barrier(world)
+        w0 = time.perf_counter()
         e0.record(stream)
         rollout(f_b, f_a, K)
         e1.record(stream)
         _barrier(world)
+        w1 = time.perf_counter()
     t_dev = e0.elapsed_time(e1) / 1e3
     t_dev = _max_over_ranks(world, t_dev)
     mlups = _job_mlups(world, cells, K, t_dev)
-    clocks = clk.summary()
+    clocks = clk.summary(w0, w1)
+    if clocks.get("sm_mhz"):
+        clocks["ms_x_median_sm_ghz"] = round(t_dev / K * 1e3 * clocks["sm_mhz"] / 1e3, 4)
+    # the state-step kernel alone: a rollout of K steps is the first step, K - 2
+    # state steps and the last step; one of 2 steps has the first and last only
+    e4 = torch.cuda.Event(enable_timing=True)
+    e5 = torch.cuda.Event(enable_timing=True)
+    rollout(f_a, f_b, 2)
+    e4.record(stream)
+    for _ in range(5):
+        rollout(f_a, f_b, 2)
+    e5.record(stream)
+    torch.cuda.synchronize()
+    t_two = e4.elapsed_time(e5) / 5 / 1e3
+    t_kernel = (t_dev - t_two) / (K - 2) if K > 2 else t_dev / K
 
     # e2e: public API, state in pinned host memory
     f_host = f_a.cpu().pin_memory()
@@ -338,15 +407,14 @@ def run_ours(args):
         torch.cuda.empty_cache()
         variants["c1"] = c1_cost(dev)
         torch.cuda.empty_cache()
-        variants["update_call"] = update_call_cost(dev)
-        torch.cuda.empty_cache()
         variants["frames"] = frames_cost(dev)
         torch.cuda.empty_cache()
         variants["precision_512"] = precision_cost(dev, args.c5_steps)
 
+    upd = update_call_cost(dev) if (rank == 0 and not args.no_variants) else None
     if rank == 0:
         peak, peak_kind = _peaks()
-        achieved = bytes_per_cell * (cells * K) / t_dev / 1e9  # per GPU
+        achieved = bytes_per_cell * cells / t_kernel / 1e9  # per GPU
         line = {
             "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS",
             "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -366,21 +434,30 @@ def run_ours(args):
                          "traffic_unit": "DRAM bytes per launch (ncu)",
                          "algorithmic_bytes_per_launch": bytes_per_cell * cells,
                          "bytes_per_cell": bytes_per_cell,
-                         "kernel": KERNEL_LABEL[args.storage]},
+                         "kernel": KERNEL_LABEL[args.storage],
+                         "kernel_ms": round(t_kernel * 1e3, 4),
+                         "kernel_ms_how": "CUDA events: (t(K-step rollout) - t(2-step "
+                                          "rollout)) / (K - 2)",
+                         "whole_rollout_frac": round(bytes_per_cell * cells * K / t_dev / 1e9
+                                                     / peak, 4)},
             "e2e": {"value": round(_job_mlups(world, cells, K, t_e2e), 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K,
                     "note": "LBMNode.run with pinned-host state in/out, per K-step rollout"},
-            "gpu_launches": K + 1,
+            # the first step (one-pass tiled kernel), K - 2 state steps, the last step
+            "gpu_launches": K,
             "clocks": clocks,
+            "update_call": upd,
+            "host": host_info(),
             "variants": variants,
         }
         if world == 1 and not args.no_cpu_baseline:
-            procs = 1
-            v, _ = cpu_baseline(procs, nx=16, steps=8)
+            procs = _host_cores()
+            v, _ = cpu_baseline(procs, nx=16, steps=4)
             line["cpu_baseline"] = {"value": round(v, 3), "unit": "MLUPS", "cores": procs,
                                     "kind": "port",
-                                    "sample": "float32 oracle restatement, 16x256x256 slab of "
-                                              "the workload, 8 steps, 1 process"}
+                                    "sample": f"{procs} processes x 16x256x256 slab of the "
+                                              "workload x 4 steps (float32 restatement of "
+                                              "the reference step; JAX absent)"}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -618,33 +695,47 @@ def c1_cost(dev, grid=(64, 64, 64), steps=500):
 
 
 def update_call_cost(dev, grid=(256, 256, 256), calls=20):
-    """One ``LBMNode.update`` call per step, as a graph manager drives the node:
-    the reference-layout state in and out of every call (a prepare pass and a
-    last pass), on the benchmark workload; mean over ``calls`` calls."""
+    """One ``LBMNode.update`` call per step, as a graph manager drives the node
+    (the reference-layout state in and out of every call), on the benchmark
+    workload; mean over ``calls`` calls.  The default one-pass tiled kernel
+    moves 173 B per cell (f in 76, wall 1, f out 76, density + velocity +
+    pressure 20); the two-pass form (collide into the workspace, then the pull
+    step) moves 324 and is timed beside it."""
     import torch
     from maddening_b200 import LBMNode
     from maddening_b200.geometry import random_spheres
-    node = LBMNode("call", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0,
-                   wall_mask=random_spheres(grid, seed=0), outlet_condition="zero_gradient",
-                   device=dev)
+    wall = random_spheres(grid, seed=0)
     bi = {"inlet_velocity": np.array(U_IN)}
-    st = node.initial_state()
-    for _ in range(3):
-        st = node.update(st, bi, 1.0)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(calls):
-        st = node.update(st, bi, 1.0)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / calls
     cells = grid[0] * grid[1] * grid[2]
-    return {"workload": "LBMNode.update, one call per step, %s" % "x".join(map(str, grid)),
-            "ms_per_call": round(ms, 4), "mlups": round(cells / ms / 1e3, 1),
-            "bytes_per_cell": 324,
-            "hbm_frac": round(cells * 324 / (ms * 1e-3) / 1e9 / _peaks()[0], 4)}
+    res = {"workload": "LBMNode.update, one call per step, %s" % "x".join(map(str, grid))}
+    for one_pass in (True, False):
+        node = LBMNode("call", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0,
+                       wall_mask=wall, outlet_condition="zero_gradient", device=dev,
+                       one_pass=one_pass)
+        st = node.initial_state()
+        for _ in range(3):
+            st = node.update(st, bi, 1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(calls):
+            st = node.update(st, bi, 1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / calls
+        bpc = 173 if one_pass else 324
+        frac = round(cells * bpc / (ms * 1e-3) / 1e9 / _peaks()[0], 4)
+        if one_pass:
+            res.update({"value": round(cells / ms / 1e3, 1), "unit": "MLUPS",
+                        "ms_per_call": round(ms, 4), "bytes_per_cell": bpc, "hbm_frac": frac,
+                        "kernel": "k_tiled<19,float,kOutAoS,faces,no force> (one pass)"})
+        else:
+            res["two_pass"] = {"value": round(cells / ms / 1e3, 1), "ms_per_call": round(ms, 4),
+                               "bytes_per_cell": bpc, "hbm_frac": frac}
+        del node, st
+        torch.cuda.empty_cache()
+    return res
 
 
 def frames_cost(dev, grid=(256, 256, 256), frames=20):
@@ -694,10 +785,10 @@ def adjoint_cost(dev):
     loss = final kinetic energy (FP32 storage)."""
     import torch
     from maddening_b200 import LBMNode
-    from oracle import lbm_ref as R  # z-wall mask helper only
+    from maddening_b200.geometry import z_walls
     grid, steps, K = (128, 128, 128), 1000, 32
     rng = np.random.default_rng(0)
-    node = LBMNode("adj", 1.0, grid_shape=grid, viscosity=0.2 / 3.0, wall_mask=R.z_walls(grid),
+    node = LBMNode("adj", 1.0, grid_shape=grid, viscosity=0.2 / 3.0, wall_mask=z_walls(grid),
                    device=dev)
     st = node.initial_state()
     F = torch.tensor(1e-6 * rng.standard_normal(grid + (3,)), dtype=torch.float32, device=dev,
@@ -755,6 +846,7 @@ def run_reference(args):
                                    "(float32 restatement of the reference step; JAX absent)"},
         "e2e": {"value": round(v, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "host": host_info(),
     }
     print(json.dumps(line), flush=True)
 

@@ -10,6 +10,8 @@
   first and last plane of axis 0, the inlet/outlet axis), radii uniform in
   [r_min, r_max], periodic in the other axes, added one at a time until the
   solid fraction reaches ``solid_fraction``.
+* ``z_walls`` -- walls on the first and last plane of the last axis (the
+  channel workloads).
 """
 
 from __future__ import annotations
@@ -82,4 +84,12 @@ def random_spheres(grid_shape, seed: int = 0, r_min: float = 4.0, r_max: float =
         view = wall.reshape(-1)
         solid += int(np.count_nonzero(~view[flat]))
         view[flat] = True
+    return wall
+
+
+def z_walls(grid_shape) -> np.ndarray:
+    """Walls on the first and last plane of the last axis (True = wall)."""
+    wall = np.zeros(tuple(int(n) for n in grid_shape), dtype=bool)
+    wall[..., 0] = True
+    wall[..., -1] = True
     return wall
