@@ -210,6 +210,37 @@ int lbm_rollout_history(const lbm_plan* plan, lbm_stream_t stream, const void* f
                         const lbm_step_args* args, const lbm_moments* out,
                         const lbm_history* history, void* workspace, size_t workspace_bytes);
 
+/* ---- Stepping the device state directly ------------------------------------
+ * For runners that step a block of a larger lattice themselves and exchange
+ * halo planes between steps (the slab-sharded runner; the reference's
+ * ShardedStencilNode around update_padded, cloud/multigpu/sharded_node.py:
+ * 345-413).  The state is what lbm_rollout keeps between steps: Q planes of
+ * the plan's cells (plane q holds population q of every cell, cells in the
+ * grid's C order) of post-collision normalised offsets in the plan's storage
+ * type, lbm_state_bytes bytes.  A "slice" is one index of reference axis 0
+ * (n1 n2 cells for D3Q19, ny for D2Q9).  Every axis is periodic in the
+ * pull, so a block padded by one slice on each side of axis 0 steps its
+ * interior correctly once its pad slices hold the neighbours' populations
+ * that cross into it (the 5 of D3Q19 / 3 of D2Q9 whose axis-0 component
+ * points inwards).  index_offset: the index of the block's first cell in the
+ * whole lattice (it seeds the stochastic rounding of 16-bit storage, so a
+ * block rounds as the whole lattice would); 0 for a whole lattice.
+ *
+ * lbm_state_from_f: state = C(f) of a reference-layout f (the first pass of a
+ *   rollout).
+ * lbm_state_step: one step (pull, wall swap, faces, collide) of the slices
+ *   [first, first + count), state_in -> state_out (not aliased); one cell per
+ *   thread for every storage form, bit-identical to the rollout's forms.
+ * lbm_state_to_f: the reference f_bc and moments of the step that pulls from
+ *   state (the last pass of a rollout). */
+int lbm_state_from_f(const lbm_plan* plan, lbm_stream_t stream, const void* f_in,
+                     void* state_out, const lbm_step_args* args, int64_t index_offset);
+int lbm_state_step(const lbm_plan* plan, lbm_stream_t stream, const void* state_in,
+                   void* state_out, const lbm_step_args* args, int64_t first, int64_t count,
+                   int64_t index_offset);
+int lbm_state_to_f(const lbm_plan* plan, lbm_stream_t stream, const void* state_in,
+                   void* f_out, const lbm_step_args* args, const lbm_moments* out);
+
 /* ---- Pipe node -----------------------------------------------------------
  * MADDENING's LBMPipeNode (src/maddening/nodes/lbm_pipe.py:393-879).
  * Single phase (G == 0): D3Q19 BGK with the Guo source of an actuator-disc

@@ -95,6 +95,11 @@ _SIGS = {
     "lbm_rollout_backward": ([_P, _P, _P, C.c_int64, C.c_int64, C.POINTER(lbm_step_args),
                               _P, _P, _P, _P, _P, _P, C.c_size_t], C.c_int),
     "lbm_reduce_workspace_bytes": ([_P, C.POINTER(C.c_size_t)], C.c_int),
+    "lbm_state_from_f": ([_P, _P, _P, _P, C.POINTER(lbm_step_args), C.c_int64], C.c_int),
+    "lbm_state_step": ([_P, _P, _P, _P, C.POINTER(lbm_step_args), C.c_int64, C.c_int64,
+                        C.c_int64], C.c_int),
+    "lbm_state_to_f": ([_P, _P, _P, _P, C.POINTER(lbm_step_args), C.POINTER(lbm_moments)],
+                       C.c_int),
     "lbm_mass_momentum": ([_P, _P, _P, _P, _P, C.c_size_t], C.c_int),
 }
 

@@ -107,6 +107,8 @@ int build_args(const lbm_plan* p, const lbm_step_args* args, const lbm_moments* 
                lbm::StepArgs* a) {
   std::memset(a, 0, sizeof(*a));
   a->g = p->g;
+  a->cell0 = 0;
+  a->cell_end = p->g.ncell;
   a->omega = 1.0 / p->tau;
   a->guo_c = 1.0 - 0.5 / p->tau;
   if (args == nullptr) return fail(LBM_ERR_INVALID, "args is NULL");
@@ -154,7 +156,7 @@ int launch_prepare(const lbm::StepArgs& a, cudaStream_t s) {
 
 template <int Q, class S, int MODE>
 void launch_step_mode(const lbm::StepArgs& a, cudaStream_t s) {
-  const unsigned grid = grid_for(a.g.ncell);
+  const unsigned grid = grid_for(a.cell_end - a.cell0);
   const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
   const bool force = a.force_mode != 0;
   if (faces) {
@@ -1071,6 +1073,102 @@ int lbm_rollout_history(const lbm_plan* p, lbm_stream_t stream, const void* f_in
     }
   }
   return fail(LBM_ERR_INVALID, "bad storage");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Stepping the device state directly (the sharded runner)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+enum StateOp { kFromF, kStep, kToF };
+
+template <int Q, class S>
+int state_op(StateOp op, const lbm::StepArgs& a, cudaStream_t s) {
+  if (op == kFromF) return launch_prepare<Q, S>(a, s);
+  if (op == kStep) {
+    launch_step_mode<Q, S, lbm::kOutState>(a, s);  // one cell per thread, any storage
+    return cuda_check(cudaGetLastError(), "k_step launch");
+  }
+  return launch_step<Q, S>(a, true, s);
+}
+
+template <int Q>
+int state_op_s(const lbm_plan* p, StateOp op, const lbm::StepArgs& a, cudaStream_t s) {
+  switch (p->storage) {
+    case LBM_STORE_F32: return state_op<Q, float>(op, a, s);
+    case LBM_STORE_F16: return state_op<Q, __half>(op, a, s);
+    case LBM_STORE_BF16: return state_op<Q, __nv_bfloat16>(op, a, s);
+    case LBM_STORE_F64: return state_op<Q, double>(op, a, s);
+  }
+  return fail(LBM_ERR_INVALID, "bad storage");
+}
+
+int run_state_op(const lbm_plan* p, lbm_stream_t stream, StateOp op, const lbm::StepArgs& a) {
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  return p->Q == 19 ? state_op_s<19>(p, op, a, s) : state_op_s<9>(p, op, a, s);
+}
+
+int state_args(const lbm_plan* p, const lbm_step_args* args, const lbm_moments* out,
+               int64_t index_offset, lbm::StepArgs* a) {
+  if (p == nullptr) return fail(LBM_ERR_INVALID, "plan is NULL");
+  if (index_offset < 0) return fail(LBM_ERR_INVALID, "index_offset must be >= 0");
+  const int rc = build_args(p, args, out, a);
+  if (rc) return rc;
+  // the rounding seed takes the index modulo 2^32, as for a whole lattice
+  a->sr_offset = static_cast<uint32_t>(static_cast<uint64_t>(index_offset));
+  return LBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_state_from_f(const lbm_plan* p, lbm_stream_t stream, const void* f_in, void* state_out,
+                     const lbm_step_args* args, int64_t index_offset) {
+  if (f_in == nullptr || state_out == nullptr)
+    return fail(LBM_ERR_INVALID, "f_in/state_out is NULL");
+  lbm::StepArgs a;
+  int rc = state_args(p, args, nullptr, index_offset, &a);
+  if (rc) return rc;
+  a.f_in = f_in;
+  a.pout = state_out;
+  return run_state_op(p, stream, kFromF, a);
+}
+
+int lbm_state_step(const lbm_plan* p, lbm_stream_t stream, const void* state_in, void* state_out,
+                   const lbm_step_args* args, int64_t first, int64_t count,
+                   int64_t index_offset) {
+  if (state_in == nullptr || state_out == nullptr)
+    return fail(LBM_ERR_INVALID, "state_in/state_out is NULL");
+  if (state_in == state_out) return fail(LBM_ERR_INVALID, "state_in must not be state_out");
+  lbm::StepArgs a;
+  int rc = state_args(p, args, nullptr, index_offset, &a);
+  if (rc) return rc;
+  if (first < 0 || count < 0 || first + count > p->shape[0])
+    return fail(LBM_ERR_INVALID, "slices [%lld, %lld) outside axis 0 of extent %lld",
+                (long long)first, (long long)(first + count), (long long)p->shape[0]);
+  if (count == 0) return LBM_OK;
+  const uint32_t slice = p->g.ncell / static_cast<uint32_t>(p->shape[0]);
+  a.cell0 = static_cast<uint32_t>(first) * slice;
+  a.cell_end = static_cast<uint32_t>(first + count) * slice;
+  a.pin = state_in;
+  a.pout = state_out;
+  return run_state_op(p, stream, kStep, a);
+}
+
+int lbm_state_to_f(const lbm_plan* p, lbm_stream_t stream, const void* state_in, void* f_out,
+                   const lbm_step_args* args, const lbm_moments* out) {
+  if (state_in == nullptr || f_out == nullptr)
+    return fail(LBM_ERR_INVALID, "state_in/f_out is NULL");
+  lbm::StepArgs a;
+  int rc = state_args(p, args, out, 0, &a);
+  if (rc) return rc;
+  a.pin = state_in;
+  a.f_out = f_out;
+  return run_state_op(p, stream, kToF, a);
 }
 
 }  // extern "C"

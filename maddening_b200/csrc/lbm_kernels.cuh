@@ -137,6 +137,12 @@ struct StepArgs {
   // non-wall cell; moments without the half-force step.
   uint32_t prop_x;
   const uint8_t* prop_mask;
+  // k_step covers cells [cell0, cell_end) of the plan (0 and ncell by default:
+  // a runner that steps a block plane range by plane range sets them).
+  uint32_t cell0, cell_end;
+  // Added to a cell's index where it seeds the stochastic rounding of 16-bit
+  // storage, so that a block of a larger lattice rounds as that lattice does.
+  uint32_t sr_offset;
 };
 
 constexpr uint32_t kMomDensityDev = 1u;
@@ -609,7 +615,7 @@ __device__ __forceinline__ Cell locate(const Geo& g, uint32_t c) {
 // the interior lattice, so that a periodic pad rounds as the unpadded lattice.
 template <int Q>
 __device__ __forceinline__ uint32_t sr_index(const StepArgs& a, const Cell& x) {
-  if (a.face_inset == 0) return x.c;
+  if (a.face_inset == 0) return x.c + a.sr_offset;
   const Geo& g = a.g;
   auto in = [](uint32_t i, uint32_t n) { return i == 0 ? n - 3 : (i + 1 == n ? 0u : i - 1); };
   const uint32_t j0 = Lat<Q>::D == 3 ? in(x.i0, g.n0) : 0u;
@@ -859,11 +865,12 @@ template <int Q, class S, int MODE, bool FACES, bool FORCE>
 __global__ void __launch_bounds__(kBlock, min_blocks<S>())
     k_step(const __grid_constant__ StepArgs a) {
   using IO = typename StoreT<S>::IO;
-  const uint32_t cidx = blockIdx.x * kBlock + threadIdx.x;
-  if (cidx < a.g.ncell) step_cell<Q, S, MODE, FACES, FORCE>(a, cidx);
+  const uint32_t first = a.cell0 + blockIdx.x * kBlock;
+  const uint32_t cidx = first + threadIdx.x;
+  if (cidx < a.cell_end) step_cell<Q, S, MODE, FACES, FORCE>(a, cidx);
   if constexpr (MODE == kOutAoS || MODE == kOutRecord) {
     if (MODE == kOutAoS || a.f_out != nullptr)
-      aos_flush<Q, IO>(static_cast<IO*>(a.f_out), blockIdx.x * kBlock, a.g.ncell);
+      aos_flush<Q, IO>(static_cast<IO*>(a.f_out), first, a.cell_end);
   }
 }
 

@@ -2,22 +2,34 @@
 
 The B200 counterpart of MADDENING's ``ShardedStencilNode`` around
 ``LBMNode.update_padded`` (``src/maddening/cloud/multigpu/sharded_node.py:116-
-420``): each rank owns a slab of the global lattice along axis 0 and keeps it
-permanently in a block padded by one halo cell per side of every spatial axis.
-Before every step the halos are refreshed --
+420``): each rank owns a slab of the global lattice along reference axis 0.
 
-* axes 1 and 2 (not sharded): periodic copies inside the block;
-* axis 0: the first and last interior planes go to the previous and next rank
-  and come back as their halo planes, whole ``(n1 + 2) x (n2 + 2) x Q``
-  planes that are contiguous in the ``(*grid, Q)`` layout, so the point-to-
-  point send/receive (NCCL between GPUs, gloo on CPU) needs no packing --
+``ShardedLBM`` keeps its slab between steps in the kernels' own state layout
+(post-collision normalised offsets, ``lbm_state_*`` of the C ABI), padded by
+one slice on each side of axis 0 only.  A step pulls every population from
+its upstream neighbour, so the first interior slice needs, from the previous
+rank's last slice, only the populations whose axis-0 component is +1 (5 of
+D3Q19, 3 of D2Q9), and the last interior slice the ones with -1 from the next
+rank.  Per step each rank therefore
 
-then ``lbm_update_padded`` advances the interior (the whole block is
-collided, the interior pulls across the halo, walls and faces act on the
-interior).  Only halo planes cross between ranks; the periodic wrap of axis 0
-joins the last rank to the first.  The lattice is periodic on every axis, as
-the reference's stream is; pressure / velocity faces may sit on axes 1 and 2
-(every slab spans them whole), not on the sharded axis 0.
+1. steps its two boundary slices (one ``lbm_state_step`` each),
+2. sends their crossing populations to the neighbours and receives theirs
+   into its pad slices (point-to-point, on a second stream with NCCL so that
+   the transfer overlaps step 3; staged through host memory with gloo),
+3. steps the interior slices, and waits for the exchange before the next step.
+
+Bytes over the link per rank and step: 2 x 5 x n1 n2 populations in the
+storage type (D3Q19 FP32 256 x 256: 2.6 MB), against 2 x 19 (n1 + 2)(n2 + 2)
+for whole halo planes; HBM traffic per step: one state step of the slab
+(152 B/cell FP32) instead of ``update_padded``'s three reference-layout
+passes.  The results equal ``LBMNode.run`` on the whole lattice bit for bit
+(16-bit storage included: each block seeds its stochastic rounding with the
+whole lattice's cell index).  Axes 1 and 2 are not split and keep their
+periodic wrap inside the kernels; pressure / velocity faces may sit on them,
+not on the sharded axis 0.
+
+``fill_halos`` refreshes a block padded on every axis in the reference layout,
+for callers of ``LBMNode.update_padded`` (the reference's own sharded path).
 """
 
 from __future__ import annotations
@@ -74,16 +86,59 @@ def fill_halos(fp: torch.Tensor, rank: int, world: int, group=None) -> None:
         req.wait()
 
 
+def crossing_populations(lattice):
+    """Indices of the populations whose reference-axis-0 component is +1 and
+    -1: the ones that cross a slab face along axis 0 in a step."""
+    e0 = np.asarray(lattice.e)[:, 0]
+    return np.nonzero(e0 == 1)[0].tolist(), np.nonzero(e0 == -1)[0].tolist()
+
+
+def exchange_slices(state: torch.Tensor, plus, minus, rank: int, world: int, group=None,
+                    staged: bool = False) -> None:
+    """Fill the pad slices of a slab state ``state`` (shape ``(Q, n + 2, slice)``,
+    slices 1..n the interior) with the neighbours' crossing populations: pad
+    slice 0 gets populations ``plus`` of the previous rank's last interior
+    slice, pad slice n + 1 populations ``minus`` of the next rank's first one
+    (periodic: rank 0's previous is the last rank).  Every rank of ``group``
+    calls it with the same shapes, in the same step; ``staged``: move the
+    messages through host memory (gloo)."""
+    n = state.shape[1] - 2
+    ip = torch.as_tensor(plus, device=state.device)
+    im = torch.as_tensor(minus, device=state.device)
+    send_next = state[ip, n]  # gathered copies, contiguous
+    send_prev = state[im, 1]
+    if world == 1:
+        state[ip, 0] = send_next
+        state[im, n + 1] = send_prev
+        return
+    if staged:
+        send_next, send_prev = send_next.cpu(), send_prev.cpu()
+    recv_prev = torch.empty_like(send_next)
+    recv_next = torch.empty_like(send_prev)
+    prev, nxt = (rank - 1) % world, (rank + 1) % world
+    gprev = dist.get_global_rank(group, prev) if group is not None else prev
+    gnext = dist.get_global_rank(group, nxt) if group is not None else nxt
+    # Point-to-point messages between two ranks match in issue order, so with
+    # two ranks (prev == next) the plus populations land in the plus buffer.
+    ops = [dist.P2POp(dist.isend, send_next, gnext, group),
+           dist.P2POp(dist.irecv, recv_prev, gprev, group),
+           dist.P2POp(dist.isend, send_prev, gprev, group),
+           dist.P2POp(dist.irecv, recv_next, gnext, group)]
+    for req in dist.batch_isend_irecv(ops):
+        req.wait()
+    state[ip, 0] = recv_prev.to(state.device)
+    state[im, n + 1] = recv_next.to(state.device)
+
+
 class ShardedLBM:
     """The rollout of a global ``LBMNode`` split into slabs along axis 0.
 
     ``node``: the global node (grid, walls, viscosity, lattice, storage, faces
-    on axes 1 / 2 only).  Rank ``r`` of ``world`` owns planes
+    on axes 1 / 2 only).  Rank ``r`` of ``world`` owns slices
     ``[r n0 / world, (r + 1) n0 / world)``; ``n0`` must divide evenly.
     ``scatter`` loads a global state (every rank passes the same one), ``run``
     advances ``n`` steps, ``local_state`` is this rank's interior, ``gather``
-    collects the global state on every rank.  With gloo the padded blocks are
-    staged through host memory for the exchange."""
+    collects the global state on every rank."""
 
     def __init__(self, node: LBMNode, group=None):
         self.node = node
@@ -97,13 +152,14 @@ class ShardedLBM:
         self.grid = grid
         self.n0 = grid[0] // self.world
         self.lo = self.rank * self.n0
-        self.pshape = (self.n0 + 2,) + tuple(n + 2 for n in grid[1:])
-        # the padded wall mask of this slab: periodic wrap on every axis
-        idx = np.arange(self.lo - 1, self.lo + self.n0 + 1) % grid[0]
-        wall = np.take(node._wall_np, idx, axis=0)
-        self._wall_pad = np.pad(wall, [(0, 0)] + [(1, 1)] * (len(grid) - 1), mode="wrap")
+        self.pshape = (self.n0 + 2,) + tuple(grid[1:])
+        self.slice = int(np.prod(grid[1:]))
+        self._rows = np.arange(self.lo - 1, self.lo + self.n0 + 1) % grid[0]
+        self._wall_pad = np.take(node._wall_np, self._rows, axis=0)
+        self._plus, self._minus = crossing_populations(node.lattice)
         self._staged = dist.is_initialized() and dist.get_backend(group) == "gloo"
-        self._bufs = None
+        self._state = None
+        self._comm = None
 
     @staticmethod
     def _check_face(face):
@@ -117,37 +173,90 @@ class ShardedLBM:
         if "outlet_pressure" in bi:
             self._check_face(self.node._outlet_face)
 
-    # -- state ---------------------------------------------------------------
     def _dev(self):
         return self.node._dev()
 
+    def _block(self, arr, dev, dtype=None):
+        """The padded slab (axis-0 rows lo - 1 .. lo + n0, periodic) of a
+        global array."""
+        t = torch.as_tensor(arr, device=dev)
+        rows = torch.as_tensor(self._rows, device=dev)
+        t = t.index_select(0, rows)
+        return (t.to(dtype) if dtype is not None else t).contiguous()
+
+    def _block_inputs(self, bi, dev):
+        out = dict(bi)
+        D = len(self.grid)
+        f = bi.get("body_force", None)
+        if f is not None and np.ndim(f) == D + 1:
+            out["body_force"] = self._block(f, dev, self.node._io_dtype)
+        if "wall_mask_update" in bi:
+            out["wall_mask_update"] = self._block(bi["wall_mask_update"], dev)
+        return out
+
+    def _view(self, t):
+        return t.view(self.node._Q, self.n0 + 2, self.slice)
+
+    def _offset(self):
+        # the whole lattice's index of the block's first cell, modulo 2^32
+        return ((self.lo - 1) * self.slice) % (1 << 32)
+
+    # -- state ---------------------------------------------------------------
     def scatter(self, state: dict) -> None:
         """Load this rank's slab of a global state (``f`` of shape (*grid, Q))."""
-        dev = self._dev()
-        f = torch.as_tensor(state["f"], device=dev).to(self.node._io_dtype)
-        Q = f.shape[-1]
-        fp = torch.zeros(self.pshape + (Q,), dtype=f.dtype, device=dev)
-        fp[1:-1][(slice(None),) + (slice(1, -1),) * (len(self.grid) - 1)] = \
-            f[self.lo: self.lo + self.n0]
-        D = len(self.grid)
-        self._bufs = {
-            "f": [fp, torch.empty_like(fp)],
-            "density": torch.zeros(self.pshape, dtype=f.dtype, device=dev),
-            "velocity": torch.zeros(self.pshape + (D,), dtype=f.dtype, device=dev),
-            "pressure": torch.zeros(self.pshape, dtype=f.dtype, device=dev),
-            "wall": torch.as_tensor(self._wall_pad.astype(np.uint8), device=dev).contiguous(),
-        }
+        node, dev = self.node, self._dev()
+        # the first collide takes the first run's boundary inputs (the force),
+        # as a rollout's does: it runs there
+        self._f_pad = self._block(state["f"], dev, node._io_dtype)
+        plan = node._padded_plan(self.pshape)
+        nbytes = plan.state_bytes()
+        self._bufs = [torch.empty(nbytes, dtype=torch.uint8, device=dev) for _ in range(2)]
         self._cur = 0
+        self._k = 0  # steps done; after k >= 1 steps the held state pulls into step k
+        self._wall = torch.as_tensor(self._wall_pad.astype(np.uint8), device=dev).contiguous()
+        self._last_bi = {}
+        self._state = True
 
-    def _interior(self, t):
-        return t[1:-1][(slice(None),) + (slice(1, -1),) * (len(self.grid) - 1)]
+    def _typed(self, buf):
+        dt = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16,
+              "f64": torch.float64}[self.node.storage]
+        return self._view(buf.view(dt))
+
+    def _exchange(self, buf):
+        exchange_slices(self._typed(buf), self._plus, self._minus, self.rank, self.world,
+                        self.group, self._staged)
 
     def local_state(self) -> dict:
-        """This rank's interior: ``f``, ``density``, ``velocity``, ``pressure``."""
-        b = self._bufs
-        return {"f": self._interior(b["f"][self._cur]), "density": self._interior(b["density"]),
-                "velocity": self._interior(b["velocity"]),
-                "pressure": self._interior(b["pressure"])}
+        """This rank's interior: ``f``, ``density``, ``velocity``, ``pressure``
+        after the steps run so far (the moments of the last step; zero before
+        the first)."""
+        if self._state is None:
+            raise RuntimeError("scatter a state first")
+        node, dev = self.node, self._dev()
+        D = len(self.grid)
+        if self._k == 0:
+            z = torch.zeros(self.pshape[1:], dtype=node._io_dtype, device=dev)
+            zeros = z.expand((self.n0,) + z.shape).contiguous()
+            return {"f": self._f_pad[1:-1].clone(), "density": zeros.clone(),
+                    "velocity": torch.zeros((self.n0,) + self.pshape[1:] + (D,),
+                                            dtype=node._io_dtype, device=dev),
+                    "pressure": zeros}
+        plan = node._padded_plan(self.pshape)
+        f = torch.empty(self.pshape + (node._Q,), dtype=node._io_dtype, device=dev)
+        rho = torch.empty(self.pshape, dtype=node._io_dtype, device=dev)
+        vel = torch.empty(self.pshape + (D,), dtype=node._io_dtype, device=dev)
+        prs = torch.empty(self.pshape, dtype=node._io_dtype, device=dev)
+        m = _lib.lbm_moments()
+        m.density, m.velocity, m.pressure = rho.data_ptr(), vel.data_ptr(), prs.data_ptr()
+        args, keep = node._step_args({"wall_mask": self._wall}, self._last_bi, dev,
+                                     shape=self.pshape)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(_lib.lib().lbm_state_to_f(plan.handle, stream,
+                                             self._bufs[self._cur].data_ptr(), f.data_ptr(),
+                                             C.byref(args), C.byref(m)))
+        del keep
+        return {"f": f[1:-1], "density": rho[1:-1], "velocity": vel[1:-1],
+                "pressure": prs[1:-1]}
 
     def gather(self) -> dict:
         """The global state on every rank (slabs concatenated along axis 0)."""
@@ -163,41 +272,58 @@ class ShardedLBM:
         return out
 
     # -- stepping --------------------------------------------------------------
-    def _exchange(self, fp):
-        if not self._staged:
-            fill_halos(fp, self.rank, self.world, self.group)
-            return
-        host = fp.cpu()
-        fill_halos(host, self.rank, self.world, self.group)
-        fp.copy_(host)
-
     def run(self, boundary_inputs: dict, n_steps: int) -> None:
-        """``n_steps`` steps: halo refresh, then the padded step, each step."""
-        if self._bufs is None:
+        """``n_steps`` steps with the same boundary inputs."""
+        if self._state is None:
             raise RuntimeError("scatter a state first")
         node, dev = self.node, self._dev()
-        boundary_inputs = boundary_inputs or {}
-        self._check_inputs(boundary_inputs)
-        b = self._bufs
-        interior = tuple(n - 2 for n in self.pshape)
+        bi = self._block_inputs(boundary_inputs or {}, dev)
+        self._check_inputs(bi)
+        n = int(n_steps)
+        if n <= 0:
+            return
+        self._last_bi = bi
         plan = node._padded_plan(self.pshape)
-        ws = torch.empty(plan.state_bytes(), dtype=torch.uint8, device=dev)
-        m = _lib.lbm_moments()
-        m.density, m.velocity = b["density"].data_ptr(), b["velocity"].data_ptr()
-        m.pressure = b["pressure"].data_ptr()
+        args, keep = node._step_args({"wall_mask": self._wall}, bi, dev, shape=self.pshape)
         lib = _lib.lib()
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        for _ in range(int(n_steps)):
-            src, dst = b["f"][self._cur], b["f"][1 - self._cur]
-            self._exchange(src)
-            state = {"f": src, "wall_mask": b["wall"]}
-            args, keep = node._step_args(state, boundary_inputs, dev, shape=self.pshape,
-                                         interior=interior)
-            _lib.check(lib.lbm_update_padded(plan.handle, stream, src.data_ptr(), dst.data_ptr(),
-                                             C.byref(args), C.byref(m), ws.data_ptr(),
-                                             ws.numel()))
-            del keep
+        main = torch.cuda.current_stream(dev)
+        if self._k == 0:
+            # the first collide (with this call's inputs); the first step's f is
+            # the pull from it, so the state is held as is after one step
+            _lib.check(lib.lbm_state_from_f(plan.handle, main.cuda_stream,
+                                            self._f_pad.data_ptr(),
+                                            self._bufs[self._cur].data_ptr(), C.byref(args),
+                                            self._offset()))
+            self._exchange(self._bufs[self._cur])
+            self._f_pad = None
+            self._k, n = 1, n - 1
+        overlap = self.world > 1 and not self._staged
+        if overlap and self._comm is None:
+            self._comm = torch.cuda.Stream(dev)
+        off, n0 = self._offset(), self.n0
+
+        def step(src, dst, first, count):
+            _lib.check(lib.lbm_state_step(plan.handle, main.cuda_stream, src.data_ptr(),
+                                          dst.data_ptr(), C.byref(args), first, count, off))
+
+        for _ in range(n):
+            src, dst = self._bufs[self._cur], self._bufs[1 - self._cur]
+            if overlap and n0 > 2:
+                step(src, dst, 1, 1)           # the boundary slices first
+                step(src, dst, n0, 1)
+                ev = torch.cuda.Event()
+                ev.record(main)
+                with torch.cuda.stream(self._comm):
+                    self._comm.wait_event(ev)
+                    self._exchange(dst)         # overlaps the interior step
+                step(src, dst, 2, n0 - 2)
+                main.wait_stream(self._comm)
+            else:
+                step(src, dst, 1, n0)
+                self._exchange(dst)
             self._cur = 1 - self._cur
+            self._k += 1
+        del keep
 
 
-__all__ = ["ShardedLBM", "fill_halos"]
+__all__ = ["ShardedLBM", "crossing_populations", "exchange_slices", "fill_halos"]

@@ -1,8 +1,9 @@
 """The slab-sharded runner (``ShardedLBM``) on the GPU: a rollout split into
-slabs along axis 0 equals the same number of ``LBMNode.update`` calls on the
-whole lattice, bit for bit -- with one rank (halos wrapped locally) and with
-two ranks sharing this GPU over gloo (halo planes staged through host memory
-between steps; no kernel waits on another rank)."""
+slabs along axis 0, kept in the kernels' state layout between steps, equals
+``LBMNode.run`` on the whole lattice bit for bit (FP32 and FP16 storage) --
+with one rank (pads filled locally), run in one call or in pieces, and with
+two ranks sharing this GPU over gloo (the crossing populations staged through
+host memory between steps; no kernel waits on another rank)."""
 
 import os
 import socket
@@ -18,36 +19,54 @@ GRID = (16, 12, 10)
 STEPS = 7
 
 
-def _setup():
+def _setup(storage="f32", grid=GRID):
     from maddening_b200 import LBMNode
     rng = np.random.default_rng(3)
-    wall = rng.random(GRID) < 0.1
-    node = LBMNode("s", 1.0, grid_shape=GRID, viscosity=0.06, wall_mask=wall,
-                   inlet_face="y_min", outlet_face="y_max")
+    wall = rng.random(grid) < 0.1
+    node = LBMNode("s", 1.0, grid_shape=grid, viscosity=0.06, wall_mask=wall,
+                   inlet_face="y_min", outlet_face="y_max", storage=storage)
     st = node.initial_state()
-    st["f"] = torch.as_tensor(node.lattice.w * (1 + 1e-3 * rng.standard_normal(GRID + (19,))),
+    st["f"] = torch.as_tensor(node.lattice.w * (1 + 1e-3 * rng.standard_normal(grid + (19,))),
                               device="cuda").float()
     bi = {"body_force": np.array([1e-5, -2e-6, 3e-6], dtype=np.float32),
           "inlet_pressure": np.float32(1 / 3 + 1e-3), "outlet_pressure": np.float32(1 / 3)}
     return node, st, bi
 
 
-def _reference(node, st, bi):
-    cur = st
-    for _ in range(STEPS):
-        cur = node.update(cur, bi, 1.0)
-    return cur
+def _reference(node, st, bi, steps=STEPS):
+    return node.run(st, bi, steps)
 
 
-def test_one_rank_equals_update_sequence():
+@pytest.mark.parametrize("grid", [GRID, (8, 12, 16)])  # rows of 16: the tiled first step
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_one_rank_equals_whole_lattice_run(storage, grid):
     from maddening_b200.sharded import ShardedLBM
-    node, st, bi = _setup()
+    node, st, bi = _setup(storage, grid)
     sh = ShardedLBM(node)
     sh.scatter(st)
     sh.run(bi, STEPS)
     out, ref = sh.gather(), _reference(node, st, bi)
     for key in ("f", "density", "velocity", "pressure"):
         assert torch.equal(out[key], ref[key]), key
+
+
+def test_run_in_pieces_equals_one_run():
+    from maddening_b200.sharded import ShardedLBM
+    node, st, bi = _setup()
+    sh = ShardedLBM(node)
+    sh.scatter(st)
+    sh.run(bi, 1)
+    sh.run(bi, 2)
+    sh.run(bi, STEPS - 3)
+    out, ref = sh.gather(), _reference(node, st, bi)
+    for key in ("f", "density", "velocity", "pressure"):
+        assert torch.equal(out[key], ref[key]), key
+    field = {"body_force": np.random.default_rng(9).uniform(
+        -1e-5, 1e-5, GRID + (3,)).astype(np.float32)}
+    sh.scatter(st)
+    sh.run(field, 4)
+    out, ref = sh.gather(), node.run(st, field, 4)
+    assert torch.equal(out["f"], ref["f"]) and torch.equal(out["velocity"], ref["velocity"])
 
 
 def test_faces_on_the_sharded_axis_are_rejected():
@@ -66,7 +85,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank(rank, port, out):
+def _rank(rank, port, out, storage):
     import torch.distributed as dist
     from datetime import timedelta
     from maddening_b200.sharded import ShardedLBM
@@ -74,7 +93,7 @@ def _rank(rank, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=2, timeout=timedelta(seconds=120))
     try:
         torch.cuda.set_device(0)
-        node, st, bi = _setup()
+        node, st, bi = _setup(storage)
         sh = ShardedLBM(node)
         sh.scatter(st)
         sh.run(bi, STEPS)
@@ -88,11 +107,12 @@ def _rank(rank, port, out):
         dist.destroy_process_group()
 
 
-def test_two_ranks_equal_update_sequence():
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_two_ranks_equal_whole_lattice_run(storage):
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, port, out, storage)) for r in range(2)]
     for p in procs:
         p.start()
     res = sorted(out.get(timeout=300) for _ in procs)
