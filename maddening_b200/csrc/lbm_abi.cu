@@ -1258,24 +1258,26 @@ int run_pipe_mp(const lbm_plan* p, cudaStream_t s, const lbm::StepArgs& a,
   m.drho = pa->rho_liquid - pa->rho_gas;
   m.psi = ws + 2 * sb;
   m.f_aos_in = f_in;
-  m.fin = A;
   const unsigned grid = grid_for(p->g.ncell);
+  // step 1: psi of the reference f, then its collide into A
   lbm::k_mp_density<R, lbm::kMPFirst><<<grid, lbm::kBlock, 0, s>>>(m);
   int rc = cuda_check(cudaGetLastError(), "k_mp_density launch");
   if (rc) return rc;
-  for (int64_t i = 0; i < n; ++i) {
+  m.fout = A;
+  lbm::k_mp_collide<R, true><<<grid, lbm::kBlock, 0, s>>>(m);
+  rc = cuda_check(cudaGetLastError(), "k_mp_collide launch");
+  if (rc) return rc;
+  // steps 2..n: both passes pull from the post-collision planes
+  for (int64_t i = 1; i < n; ++i) {
     m.fin = A;
     m.fout = B;
-    lbm::k_mp_collide<R><<<grid, lbm::kBlock, 0, s>>>(m);
+    lbm::k_mp_density<R, lbm::kMPStep><<<grid, lbm::kBlock, 0, s>>>(m);
+    rc = cuda_check(cudaGetLastError(), "k_mp_density launch");
+    if (rc) return rc;
+    lbm::k_mp_collide<R, false><<<grid, lbm::kBlock, 0, s>>>(m);
     rc = cuda_check(cudaGetLastError(), "k_mp_collide launch");
     if (rc) return rc;
     std::swap(A, B);
-    if (i + 1 < n) {
-      m.fin = A;
-      lbm::k_mp_density<R, lbm::kMPStep><<<grid, lbm::kBlock, 0, s>>>(m);
-      rc = cuda_check(cudaGetLastError(), "k_mp_density launch");
-      if (rc) return rc;
-    }
   }
   m.fin = A;
   m.f_aos_out = f_out;

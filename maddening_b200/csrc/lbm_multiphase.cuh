@@ -12,18 +12,19 @@
 //              (rho_liquid - rho_gas), 0, 1) (0 in walls); tracer_f passes through.
 //
 // The force at x needs psi at the 18 neighbours, i.e. the density of every
-// cell before any cell collides, so a step is two passes over populations
-// kept PRE-collision in FP32 (FP64 for FP64 plans) planes, one per direction:
-//   k_mp_density  reads f, applies the floor (rewriting the rare floored cell),
-//                 writes psi (one plane);
-//   k_mp_collide  reads f and psi of the neighbours, collides, and pushes
-//                 population q to y = x + e_q.
-// The planes hold the STREAMED populations f_str; the wall swap is deferred to
-// the readers: a wall cell's slots q and opp(q) are exchanged in registers when
-// the cell is loaded (the density is a permutation-invariant sum, and the
-// floor scales every slot alike), so the push needs no wall test at the
-// destination.  The first pass stores its input (the reference's f_bc) with
-// the same exchange, the last pass undoes it for the output.
+// cell before any cell collides, so a step is two passes over planes that
+// hold the POST-collision populations p (FP32, FP64 for FP64 plans), one per
+// direction, both pulling f_str(x)_q = p_q(x - e_q) as the single-phase step
+// does:
+//   k_mp_density  pulls, sums, applies the density floor, writes psi (one
+//                 plane);
+//   k_mp_collide  pulls again, applies the same floor, swaps wall cells,
+//                 collides with psi of the neighbours and stores p(x) in
+//                 place: every warp store is one aligned 128-byte run.
+// The first step collides the reference f (read through shared memory in
+// its (grid, 19) layout); the last pass pulls the state into the reference
+// f_bc and the outputs.  Every sum runs in the order of the push form this
+// replaced (f_str before the wall swap), so the outputs are bit-identical.
 // Traffic per cell and step: 19 loads + 1 psi store, then 19 loads + 19
 // stores + the psi loads (mostly cache hits).
 #pragma once
@@ -100,45 +101,70 @@ __device__ __forceinline__ R psi_of(R rho, R rho0) {
   return mul_r(rho0, -expm1_r(div_r(-rho, rho0)));
 }
 
-// row: the cell's reference values (first pass; a tile row filled by aos_fill).
+// Offsets of the periodic neighbours x -/+ 1 along each axis.
+struct MPNbr {
+  int32_t o0m, o0p, o1m, o1p, o2m, o2p;
+};
+
+__device__ __forceinline__ MPNbr mp_nbr(const Geo& g, const Cell& x) {
+  const int32_t pl = static_cast<int32_t>(g.plane), rw = static_cast<int32_t>(g.n2);
+  MPNbr o;
+  o.o0m = x.i0 == 0 ? (static_cast<int32_t>(g.n0) - 1) * pl : -pl;
+  o.o0p = x.i0 + 1 == g.n0 ? -(static_cast<int32_t>(g.n0) - 1) * pl : pl;
+  o.o1m = x.i1 == 0 ? (static_cast<int32_t>(g.n1) - 1) * rw : -rw;
+  o.o1p = x.i1 + 1 == g.n1 ? -(static_cast<int32_t>(g.n1) - 1) * rw : rw;
+  o.o2m = x.k == 0 ? rw - 1 : -1;
+  o.o2p = x.k + 1 == g.n2 ? 1 - rw : 1;
+  return o;
+}
+
+// The cell x + s e_q (s = +1 or -1), periodic.
+__device__ __forceinline__ uint32_t mp_at(const MPNbr& o, uint32_t c, int q, int s) {
+  const int e0 = s * Lat<19>::c0(q), e1 = s * Lat<19>::c1(q), e2 = s * Lat<19>::c2(q);
+  int32_t d = 0;
+  if (e0) d += e0 > 0 ? o.o0p : o.o0m;
+  if (e1) d += e1 > 0 ? o.o1p : o.o1m;
+  if (e2) d += e2 > 0 ? o.o2p : o.o2m;
+  return static_cast<uint32_t>(static_cast<int32_t>(c) + d);
+}
+
+// f_str of cell c: population q pulled from x - e_q of the post-collision planes.
+template <class R>
+__device__ __forceinline__ void mp_pull(const MPArgs& a, const MPNbr& o, uint32_t c, R (&f)[19]) {
+  const R* fi = static_cast<const R*>(a.fin);
+  const uint32_t n = a.s.g.ncell;
+#pragma unroll
+  for (int q = 0; q < 19; ++q) f[q] = __ldg(fi + static_cast<size_t>(q) * n + mp_at(o, c, q, -1));
+}
+
+// The floor of lbm_pipe.py:838-848 on the pulled populations f (sum s0):
+// scaled by 0.01 / s0 when s0 < 0.01; returns the sum the step continues with.
+template <class R>
+__device__ __forceinline__ R mp_floor(R (&f)[19], R s0) {
+  const R floor = static_cast<R>(0.01);
+  if (!(s0 < floor)) return s0;
+  const R ratio = div_r(floor, s0 > R(1e-20) ? s0 : R(1e-20));
+#pragma unroll
+  for (int q = 0; q < 19; ++q) f[q] = mul_r(f[q], ratio);
+  return sum19(f);
+}
+
+// Density pass of cell c.  kMPFirst: f is the reference f_bc (row of the
+// staged tile), psi without a floor; kMPStep: f pulled, floor, psi;
+// kMPLast: f pulled, floor, the reference f_bc and the outputs.
 template <class R, int MODE>
-__device__ __forceinline__ void density_cell(const MPArgs& a, uint32_t c, const R* row) {
-  const Geo& g = a.s.g;
-  R f[19];
-  if (MODE == kMPFirst) {
-#pragma unroll
-    for (int q = 0; q < 19; ++q) f[q] = row[q];
-  } else {
-    const R* fi = static_cast<const R*>(a.fin);
-#pragma unroll
-    for (int q = 0; q < 19; ++q) f[q] = fi[static_cast<size_t>(q) * g.ncell + c];
-  }
+__device__ __forceinline__ void density_cell(const MPArgs& a, uint32_t c, R (&f)[19]) {
   const bool wall = a.s.wall != nullptr && a.s.wall[c] != 0;
-  const R s0 = sum19(f);  // the new density before the floor
+  const R s0 = sum19(f);  // the new density before the floor (f_str order)
   R m[3] = {0, 0, 0};
   if (MODE == kMPLast) {
     if (wall) swap_opp(f);  // to f_bc (no velocity is taken in walls)
     else mom19(f, m);       // the output velocity is taken before the floor
   }
   R s = s0, rho_out = s0;
-  const R floor = static_cast<R>(0.01);
-  if (MODE != kMPFirst && s0 < floor) {  // lbm_pipe.py:838-848
-    const R ratio = div_r(floor, s0 > R(1e-20) ? s0 : R(1e-20));
-#pragma unroll
-    for (int q = 0; q < 19; ++q) f[q] = mul_r(f[q], ratio);
-    if (MODE == kMPStep) {
-      R* fo = static_cast<R*>(const_cast<void*>(a.fin));
-#pragma unroll
-      for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + c] = f[q];
-    }
-    rho_out = floor;
-    s = sum19(f);  // what the next step sums for this cell
-  }
-  if (MODE == kMPFirst) {
-    if (wall) swap_opp(f);  // f_bc -> the streamed form the planes hold
-    R* fo = static_cast<R*>(const_cast<void*>(a.fin));
-#pragma unroll
-    for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + c] = f[q];
+  if (MODE != kMPFirst && s0 < static_cast<R>(0.01)) {
+    s = mp_floor(f, s0);
+    rho_out = static_cast<R>(0.01);
   }
   if constexpr (MODE != kMPLast) {
     static_cast<R*>(a.psi)[c] =
@@ -166,50 +192,54 @@ template <class R, int MODE>
 __global__ void __launch_bounds__(kBlock) k_mp_density(const MPArgs a) {
   const Geo& g = a.s.g;
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  R f[19];
   // the first and last passes stage the reference layout: every thread of
   // the block reaches the tile's barriers
-  if constexpr (MODE == kMPLast) {
-    if (c < g.ncell) density_cell<R, MODE>(a, c, nullptr);
-    aos_flush<19, R>(static_cast<R*>(a.f_aos_out), blockIdx.x * kBlock, g.ncell);
-  } else if constexpr (MODE == kMPFirst) {
+  if constexpr (MODE == kMPFirst) {
     const R* row = aos_fill<19, R>(static_cast<const R*>(a.f_aos_in), blockIdx.x * kBlock, g.ncell);
-    if (c < g.ncell) density_cell<R, MODE>(a, c, row);
-  } else if (c < g.ncell) {
-    density_cell<R, MODE>(a, c, nullptr);
+    if (c < g.ncell) {
+#pragma unroll
+      for (int q = 0; q < 19; ++q) f[q] = row[q];
+      density_cell<R, MODE>(a, c, f);  // (a wall cell's psi is psi_wall: no order issue)
+    }
+  } else {
+    if (c < g.ncell) {
+      const Cell x = locate(g, c);
+      mp_pull<R>(a, mp_nbr(g, x), c, f);
+      density_cell<R, MODE>(a, c, f);
+    }
+    if constexpr (MODE == kMPLast)
+      aos_flush<19, R>(static_cast<R*>(a.f_aos_out), blockIdx.x * kBlock, g.ncell);
   }
 }
 
-// Collide with the Shan-Chen force and exact-difference forcing, then push.
-template <class R>
+// Collide with the Shan-Chen force and exact-difference forcing; the cell's
+// own p is stored in place.  FIRST: the populations come from the reference
+// f_bc (staged tile), no floor.
+template <class R, bool FIRST>
 __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   const Geo& g = a.s.g;
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  R f[19];
+  const R* row = nullptr;
+  if constexpr (FIRST)
+    row = aos_fill<19, R>(static_cast<const R*>(a.f_aos_in), blockIdx.x * kBlock, g.ncell);
   if (c >= g.ncell) return;
   const Cell x = locate(g, c);
-  const R* fi = static_cast<const R*>(a.fin);
-  R f[19];
-#pragma unroll
-  for (int q = 0; q < 19; ++q) f[q] = fi[static_cast<size_t>(q) * g.ncell + c];
+  const MPNbr o = mp_nbr(g, x);
   const uint8_t* wm = a.s.wall;
   const bool wall = wm != nullptr && wm[c] != 0;
-  const R rho = sum19(f);  // in the order of the density pass: the same value
-  if (wall) swap_opp(f);   // the deferred wall-node swap
-  // offsets of the periodic neighbours along each axis
-  const int32_t pl = static_cast<int32_t>(g.plane), rw = static_cast<int32_t>(g.n2);
-  const int32_t o0m = x.i0 == 0 ? (static_cast<int32_t>(g.n0) - 1) * pl : -pl;
-  const int32_t o0p = x.i0 + 1 == g.n0 ? -(static_cast<int32_t>(g.n0) - 1) * pl : pl;
-  const int32_t o1m = x.i1 == 0 ? (static_cast<int32_t>(g.n1) - 1) * rw : -rw;
-  const int32_t o1p = x.i1 + 1 == g.n1 ? -(static_cast<int32_t>(g.n1) - 1) * rw : rw;
-  const int32_t o2m = x.k == 0 ? rw - 1 : -1;
-  const int32_t o2p = x.k + 1 == g.n2 ? 1 - rw : 1;
-  auto nb = [&](int q) -> uint32_t {
-    const int e0 = Lat<19>::c0(q), e1 = Lat<19>::c1(q), e2 = Lat<19>::c2(q);
-    int32_t o = 0;
-    if (e0) o += e0 > 0 ? o0p : o0m;
-    if (e1) o += e1 > 0 ? o1p : o1m;
-    if (e2) o += e2 > 0 ? o2p : o2m;
-    return static_cast<uint32_t>(static_cast<int32_t>(c) + o);
-  };
+  R rho;
+  if constexpr (FIRST) {
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = row[q];
+    if (wall) swap_opp(f);  // the f_str order of the sum
+    rho = sum19(f);
+  } else {
+    mp_pull<R>(a, o, c, f);
+    rho = mp_floor(f, sum19(f));
+  }
+  if (wall) swap_opp(f);  // the wall-node swap: f_bc
   R m[3];
   mom19(f, m);
   const R inv_den = rcp_r(rho > R(1e-10) ? rho : R(1e-10));
@@ -225,7 +255,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
 #pragma unroll
     for (int q = 1; q < 19; ++q) {
       const int e0 = Lat<19>::c0(q), e1 = Lat<19>::c1(q), e2 = Lat<19>::c2(q);
-      const R p = __ldg(psi + nb(q));
+      const R p = __ldg(psi + mp_at(o, c, q, 1));
       R(&acc)[3] = q <= 6 ? s1 : s2;
       if (e0) acc[0] = e0 > 0 ? add_r(acc[0], p) : sub_r(acc[0], p);
       if (e1) acc[1] = e1 > 0 ? add_r(acc[1], p) : sub_r(acc[1], p);
@@ -252,6 +282,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   const R usq_s = fma_r(us[0], us[0], fma_r(us[1], us[1], mul_r(us[2], us[2])));
   const R dusq = sub_r(usq_s, usq_b);
   const R r36 = mul_r(rho, static_cast<R>(1.0 / 36.0));
+  R* fo = static_cast<R*>(a.fout);
 #pragma unroll
   for (int q = 0; q < 19; ++q) {
     const R wr = mul_r(static_cast<R>(Lat<19>::wr(q)), r36);  // w_q rho
@@ -263,11 +294,8 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
     const R de = sub_r(es, eb);
     const R dfeq =
         mul_r(wr, fma_r(de, fma_r(R(4.5), add_r(es, eb), R(3)), mul_r(R(-1.5), dusq)));
-    f[q] = add_r(fma_r(-omega, sub_r(f[q], feq), f[q]), dfeq);
+    fo[static_cast<size_t>(q) * g.ncell + c] = add_r(fma_r(-omega, sub_r(f[q], feq), f[q]), dfeq);
   }
-  R* fo = static_cast<R*>(a.fout);
-#pragma unroll
-  for (int q = 0; q < 19; ++q) fo[static_cast<size_t>(q) * g.ncell + nb(q)] = f[q];
 }
 
 }  // namespace lbm
