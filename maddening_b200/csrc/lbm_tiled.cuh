@@ -56,8 +56,8 @@ template <>
 struct Sweep<19> {
   static constexpr int TY = 8, TZ = 32;  // tile rows (a1) x row cells (a2)
   static constexpr int HR = 1;           // halo rows
-  static constexpr int NCW = 6;          // collide warps, two cells per lane:
-  static constexpr int CPL = 2;          //   (8 + 2) x (32 + 2) = 340 <= 6 x 32 x 2
+  static constexpr int NCW = 7;          // collide warps, two cells per lane over the
+  static constexpr int CPL = 2;          //   (8 + 2) x 40 buffered cells <= 7 x 32 x 2
   static constexpr int MINB = 1;         // resident blocks per SM
   __host__ __device__ static constexpr int cs(int q) { return Lat<19>::c0(q); }  // sweep
   __host__ __device__ static constexpr int cr(int q) { return Lat<19>::c1(q); }  // rows
@@ -66,7 +66,7 @@ template <>
 struct Sweep<9> {
   static constexpr int TY = 1, TZ = 128;
   static constexpr int HR = 0;
-  static constexpr int NCW = 3;  // 130 cells <= 3 x 32 x 2
+  static constexpr int NCW = 3;  // 136 buffered cells <= 3 x 32 x 2
   static constexpr int CPL = 2;
   static constexpr int MINB = 2;
   __host__ __device__ static constexpr int cs(int q) { return Lat<9>::c1(q); }
@@ -88,7 +88,9 @@ struct TileShape {
   static constexpr int NOW = TY * TZ / 32;            // output warps (32 cells each)
   static constexpr int NT = 32 * (1 + NCW + NOW);     // + the producer warp
   static_assert(TZ % 32 == 0, "an output warp covers 32 cells of one tile row");
-  static_assert(32 * NCW * CPL >= RP * CW, "CPL collided cells per collide lane and plane");
+  // collide lanes walk every buffered cell (row pitch W), so the 32 cells of
+  // a warp access are consecutive in shared memory: no bank conflicts
+  static_assert(32 * NCW * CPL >= RP * W, "CPL buffered cells per collide lane and plane");
 };
 
 // Barriers and flags of a block, after the slots and the staging rows.
@@ -370,16 +372,18 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
     }
   } else if (warp <= static_cast<uint32_t>(T::NCW)) {
     // ---- collide warps: plane P in place once it has landed; lane cells
-    // m_k = lane + 32 (warp - 1 + k NCW), k < CPL, their loads issued together
+    // m_k = lane + 32 (warp - 1 + k NCW), k < CPL, of the buffered cells (row
+    // pitch W; the collided ones are columns kTileHalo - 1 .. kTileHalo + TZ),
+    // their loads issued together
     using T2 = TileShape<Q>;
     uint32_t soff[T2::CPL], rr[T2::CPL], cc[T2::CPL], rz[T2::CPL];
     bool mine[T2::CPL];
 #pragma unroll
     for (int k = 0; k < T2::CPL; ++k) {
       const uint32_t m = (warp - 1 + k * T2::NCW) * 32 + lane;
-      rr[k] = m / T::CW;
-      cc[k] = m % T::CW;
-      soff[k] = (rr[k] * T::W + kTileHalo - 1 + cc[k]) * Q;  // its place in a slot
+      rr[k] = m / T::W;
+      cc[k] = m % T::W - (kTileHalo - 1);  // wraps above CW for the unused columns
+      soff[k] = m * Q;                      // its place in a slot
       mine[k] = false;
       rz[k] = 0;
     }
