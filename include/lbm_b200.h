@@ -81,11 +81,8 @@ typedef struct {
 } lbm_face_bc;
 
 /* lbm_desc.flags */
-#define LBM_PLAN_STAGED_ROWS 1u /* rollout steps stage neighbour rows in shared
-                                   memory with bulk async copies (rows of >= 128
-                                   cells and a multiple of 16 bytes); slower than
-                                   the default global gather on B200, kept for
-                                   comparison */
+/* bit 1u is reserved (an earlier row-staged rollout step, slower than the
+   default gather, was removed) and rejected by lbm_plan_create */
 #define LBM_PLAN_SINGLE_CELLS 2u /* rollout steps update one cell per thread
                                    (FP16/BF16 storage otherwise takes the
                                    four-cell step on rows of a multiple of 256

@@ -35,7 +35,6 @@ class LbmError(RuntimeError):
         self.status = status
 
 
-PLAN_STAGED_ROWS = 1
 PLAN_SINGLE_CELLS = 2
 PLAN_PAIRED_CELLS = 4
 PLAN_TWO_PASS = 8

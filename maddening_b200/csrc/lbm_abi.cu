@@ -175,58 +175,6 @@ int launch_step(const lbm::StepArgs& a, bool final_aos, cudaStream_t s) {
   return cuda_check(cudaGetLastError(), "k_step launch");
 }
 
-// Row-staged state step (lbm_staged.cuh, opt-in LBM_PLAN_STAGED_ROWS): shape
-// and shared memory per storage; rows shorter than 128 cells keep the gather.
-template <class S>
-constexpr int staged_stages() { return sizeof(S) == 2 ? 3 : 2; }
-
-template <int Q, class S>
-bool staged_ok(const lbm_plan* p) {
-  const size_t row = static_cast<size_t>(p->g.n2) * sizeof(S);
-  const size_t smem = staged_stages<S>() * static_cast<size_t>(Q) * row + 64;
-  return (p->flags & LBM_PLAN_STAGED_ROWS) != 0 && row % 16 == 0 && p->g.n2 >= 128 &&
-         smem <= 200 * 1024;
-}
-
-template <int Q, class S, bool FACES, bool FORCE, int T>
-int launch_staged_t(const lbm::StepArgs& a, cudaStream_t s) {
-  auto kern = lbm::k_step_staged<Q, S, FACES, FORCE, T>;
-  const int stages = staged_stages<S>();
-  const size_t smem = static_cast<size_t>(stages) * Q * a.g.n2 * sizeof(S) + 64;
-  int rc = cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(smem)),
-                      "cudaFuncSetAttribute");
-  if (rc) return rc;
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem),
-                  "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-  if (rc) return rc;
-  if (per_sm < 1) per_sm = 1;
-  const uint32_t nrows = a.g.n0 * a.g.n1;
-  uint32_t grid = static_cast<uint32_t>(per_sm) * static_cast<uint32_t>(sms);
-  if (grid > nrows) grid = nrows;
-  kern<<<grid, T, smem, s>>>(a, stages);
-  return cuda_check(cudaGetLastError(), "k_step_staged launch");
-}
-
-template <int Q, class S>
-int launch_staged(const lbm::StepArgs& a, cudaStream_t s) {
-  const bool faces = a.face[0].kind != lbm::kFaceNone || a.face[1].kind != lbm::kFaceNone;
-  const bool force = a.force_mode != 0;
-  if (a.g.n2 >= 256) {
-    if (faces) return force ? launch_staged_t<Q, S, true, true, 256>(a, s)
-                            : launch_staged_t<Q, S, true, false, 256>(a, s);
-    return force ? launch_staged_t<Q, S, false, true, 256>(a, s)
-                 : launch_staged_t<Q, S, false, false, 256>(a, s);
-  }
-  if (faces) return force ? launch_staged_t<Q, S, true, true, 128>(a, s)
-                          : launch_staged_t<Q, S, true, false, 128>(a, s);
-  return force ? launch_staged_t<Q, S, false, true, 128>(a, s)
-               : launch_staged_t<Q, S, false, false, 128>(a, s);
-}
-
 // Paired-cell state step (lbm_pair.cuh): the default for 16-bit storage,
 // opt-in for FP32 (LBM_PLAN_PAIRED_CELLS), off with LBM_PLAN_SINGLE_CELLS.
 // Rows of even length (row segments when they split into warps of 64 cells,
@@ -430,8 +378,9 @@ bool tiled_ok(const lbm_plan* p, const lbm::StepArgs& a, const void* ws, bool ao
   }
 }
 
-// Runs prepare + (n - 1) state steps + final step; ws holds 1 or 2 state copies
-// (with n > 1 also the status word after them).
+// Runs the first step (one-pass tiled kernel, or prepare + a state step),
+// the state steps and the final step; ws holds 1 or 2 state copies (with n > 1
+// also the status word after them).
 template <int Q, class S>
 int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_in, void* f_out,
               int64_t n, char* ws) {
@@ -453,10 +402,8 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   a.pout = A;
   lbm::StepArgs m = a;  // the first pass and intermediate steps write no moments
   m.rho = m.vel = m.prs = nullptr;
-  // The bulk copies need 16-byte aligned rows: the caller's workspace too.
-  const bool staged = n > 1 && staged_ok<Q, S>(p) && reinterpret_cast<uintptr_t>(ws) % 16 == 0;
   const bool tiled = n > 1 && tiled_ok<S>(p, a, ws + 2 * sb, false);
-  if (staged || tiled) {
+  if (tiled) {
     m.status = reinterpret_cast<int*>(ws + 2 * sb);
     rc = cuda_check(cudaMemsetAsync(m.status, 0, sizeof(int), s), "cudaMemsetAsync");
     if (rc) return rc;
@@ -473,7 +420,7 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   for (int64_t i = 0; i + 1 < n; ++i) {
     m.pin = A;
     m.pout = B;
-    rc = staged ? launch_staged<Q, S>(m, s) : launch_state_step<Q, S>(p, m, s);
+    rc = launch_state_step<Q, S>(p, m, s);
     if (rc) return rc;
     char* t = A;
     A = B;
@@ -929,6 +876,11 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
     return fail(LBM_ERR_INVALID, "unknown storage %d", desc->storage);
   if (!(desc->tau > 0.5) || !std::isfinite(desc->tau))
     return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g). Increase viscosity.", desc->tau);
+  constexpr uint32_t kKnownFlags = LBM_PLAN_SINGLE_CELLS | LBM_PLAN_PAIRED_CELLS |
+                                   LBM_PLAN_TWO_PASS | LBM_PLAN_TEST_WAIT_TIMEOUT;
+  if (desc->flags & ~kKnownFlags)
+    return fail(LBM_ERR_INVALID, "unknown or reserved plan flags 0x%x",
+                static_cast<unsigned>(desc->flags & ~kKnownFlags));
   lbm_plan* p = new lbm_plan();
   p->Q = desc->lattice;
   p->D = desc->lattice == LBM_D3Q19 ? 3 : 2;

@@ -96,8 +96,8 @@ class LBMNode(SimulationNode):
                  wall_mask: Optional[np.ndarray] = None, inlet_face: str = "x_min",
                  outlet_face: str = "x_max", geometry_source: Optional[str] = None,
                  *, outlet_condition: str = "pressure", storage: str = "f32",
-                 device=None, staged_rows: bool = False,
-                 cells_per_thread: Optional[int] = None, one_pass: bool = True):
+                 device=None, cells_per_thread: Optional[int] = None,
+                 one_pass: bool = True):
         lat = by_name(lattice)
         if len(grid_shape) != lat.D:
             raise ValueError(f"grid_shape has {len(grid_shape)} dims but lattice "
@@ -145,7 +145,7 @@ class LBMNode(SimulationNode):
         self._wall_dev = {}
         if cells_per_thread not in (None, 1, 2):
             raise ValueError(f"cells_per_thread must be None, 1 or 2 (got {cells_per_thread})")
-        flags = _lib.PLAN_STAGED_ROWS if staged_rows else 0
+        flags = 0
         if cells_per_thread == 1:
             flags |= _lib.PLAN_SINGLE_CELLS
         elif cells_per_thread == 2:
