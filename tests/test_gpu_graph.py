@@ -32,3 +32,37 @@ def test_captured_rollout_equals_plain(storage):
         torch.cuda.synchronize()
         for key in ("f", "density", "velocity", "pressure"):
             assert torch.equal(out[key], ref[key]), key
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_captured_update_calls_equal_plain(storage):
+    """Three chained ``update`` calls (the one-pass kernel: the call a graph
+    manager makes each step) captured once and replayed give the plain calls'
+    bytes."""
+    from maddening_b200 import LBMNode
+    grid = (20, 16, 36)
+    rng = np.random.default_rng(2)
+    node = LBMNode("u", 1.0, grid_shape=grid, viscosity=0.05, wall_mask=rng.random(grid) < 0.1,
+                   outlet_condition="zero_gradient", storage=storage)
+    bi = {"inlet_velocity": np.array([0.04, 0.0, 0.0], dtype=np.float32)}
+    st = node.initial_state()
+
+    def three(s):
+        for _ in range(3):
+            s = node.update(s, bi, 1.0)
+        return s
+
+    ref = three(st)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        three(st)
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        out = three(st)
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        for key in ("f", "density", "velocity", "pressure"):
+            assert torch.equal(out[key], ref[key]), key
