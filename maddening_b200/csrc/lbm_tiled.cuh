@@ -23,10 +23,10 @@
 //     output warps, one per 32-cell tile row, pull the collided populations of
 //     plane P from slots P - 1, P, P + 1 once P + 1 is collided, apply the
 //     wall swap and the faces, take the moments and write f_bc (kOutAoS:
-//     staged per warp in shared memory and written by a bulk asynchronous
-//     store) or collide again and write the next state planes (kOutState: the
-//     first step of a rollout).  Collide warps run up to a few planes ahead of
-//     the output warps.
+//     staged per warp in shared memory, then written as whole 16-byte groups
+//     of the warp's contiguous run) or collide again and write the next state
+//     planes (kOutState: the first step of a rollout).  Collide warps run up
+//     to a few planes ahead of the output warps.
 //   * A persistent grid walks work items (column, chunk of planes along the
 //     sweep); blocks take items with a grid stride in chunk-major order, so
 //     neighbouring columns are swept at the same time and the halo rows they
@@ -88,6 +88,7 @@ struct TileShape {
   static constexpr int NOW = TY * TZ / 32;            // output warps (32 cells each)
   static constexpr int NT = 32 * (1 + NCW + NOW);     // + the producer warp
   static_assert(TZ % 32 == 0, "an output warp covers 32 cells of one tile row");
+  static_assert(RP <= 32, "one producer lane per buffered row");
   // collide lanes walk every buffered cell (row pitch W), so the 32 cells of
   // a warp access are consecutive in shared memory: no bank conflicts
   static_assert(32 * NCW * CPL >= RP * W, "CPL buffered cells per collide lane and plane");
@@ -157,38 +158,40 @@ __device__ __forceinline__ uint32_t plane_s(const TileGeo& t, const PlaneRef& p)
   return wrapu(static_cast<int>(p.k0 + p.j) - 1, t.NS);
 }
 
-// Producer thread: arm `bar` and copy one plane (tile rows with their halo)
-// into buf.
+// Producer warp: lane 0 arms `bar` with the bytes of one plane (tile rows with
+// their halo), then lane rr copies buffered row rr into buf, so the copies of a
+// plane are issued together rather than one after another.
 template <int Q>
 __device__ __forceinline__ void tiled_issue(const StepArgs& a, const TileGeo& t,
-                                            const PlaneRef& p, float* buf, uint64_t* bar) {
+                                            const PlaneRef& p, float* buf, uint64_t* bar,
+                                            uint32_t lane) {
   using T = TileShape<Q>;
   const uint32_t ps = plane_s(t, p);
   const uint32_t nrow = p.tyv + 2 * T::HR;
   constexpr uint32_t cellb = Q * 4;
-  mbar_arrive_expect_tx(bar, nrow * (p.tzv + 2 * kTileHalo) * cellb);
-  if (t.no_copy) return;
+  if (lane == 0) mbar_arrive_expect_tx(bar, nrow * (p.tzv + 2 * kTileHalo) * cellb);
+  __syncwarp();
+  const uint32_t rr = lane;
+  if (t.no_copy || rr >= nrow) return;
   const float* f = static_cast<const float*>(a.f_in);
   const uint32_t n2 = a.g.n2;
-  for (uint32_t rr = 0; rr < nrow; ++rr) {
-    const uint32_t r = wrapu(static_cast<int>(p.y0 + rr) - T::HR, t.NR);
-    const size_t rowc = static_cast<size_t>(ps) * t.SS + static_cast<size_t>(r) * t.SR;
-    float* dst = buf + static_cast<size_t>(rr) * T::W * Q;
-    uint32_t col = 0;  // buffer cell of the next copy
-    uint32_t z = p.z0 - kTileHalo;
-    if (p.z0 == 0) {  // left halo group wraps to the end of the row
-      bulk_copy_g2s(dst, f + (rowc + n2 - kTileHalo) * Q, kTileHalo * cellb, bar);
-      col = kTileHalo;
-      z = 0;
-    }
-    const bool wrap_r = p.z0 + p.tzv == n2;
-    const uint32_t zend = wrap_r ? n2 : p.z0 + p.tzv + kTileHalo;
-    bulk_copy_g2s(dst + static_cast<size_t>(col) * Q, f + (rowc + z) * Q, (zend - z) * cellb,
-                  bar);
-    if (wrap_r)  // right halo group wraps to the start of the row
-      bulk_copy_g2s(dst + static_cast<size_t>(kTileHalo + p.tzv) * Q, f + rowc * Q,
-                    kTileHalo * cellb, bar);
+  const uint32_t r = wrapu(static_cast<int>(p.y0 + rr) - T::HR, t.NR);
+  const size_t rowc = static_cast<size_t>(ps) * t.SS + static_cast<size_t>(r) * t.SR;
+  float* dst = buf + static_cast<size_t>(rr) * T::W * Q;
+  uint32_t col = 0;  // buffer cell of the next copy
+  uint32_t z = p.z0 - kTileHalo;
+  if (p.z0 == 0) {  // left halo group wraps to the end of the row
+    bulk_copy_g2s(dst, f + (rowc + n2 - kTileHalo) * Q, kTileHalo * cellb, bar);
+    col = kTileHalo;
+    z = 0;
   }
+  const bool wrap_r = p.z0 + p.tzv == n2;
+  const uint32_t zend = wrap_r ? n2 : p.z0 + p.tzv + kTileHalo;
+  bulk_copy_g2s(dst + static_cast<size_t>(col) * Q, f + (rowc + z) * Q, (zend - z) * cellb,
+                bar);
+  if (wrap_r)  // right halo group wraps to the start of the row
+    bulk_copy_g2s(dst + static_cast<size_t>(kTileHalo + p.tzv) * Q, f + rowc * Q,
+                  kTileHalo * cellb, bar);
 }
 
 // p = C(f) of the reference state of cell c (k_prepare's arithmetic), with the
@@ -255,29 +258,51 @@ __device__ __forceinline__ void face_zero_gradient_ref(float (&d)[Q], const Step
 }
 
 // Wall swap and faces of a pulled cell (apply_bc with the zero-gradient
-// neighbour taken from the reference state).
+// neighbour taken from the reference state).  The swap is a select on every
+// pair and the faces are entered only when a cell of the warp lies on one:
+// fewer branches in the output warps' path than apply_bc's.
 template <int Q, class S, bool FACES, bool FORCE>
 __device__ __forceinline__ void apply_bc_ref(const StepArgs& a, const Cell& x, bool wall,
                                              float (&d)[Q]) {
-  if (__any_sync(__activemask(), wall)) {
-    if (wall) wall_swap<Q>(d);
+#pragma unroll
+  for (int q = 1; q < Q; ++q) {
+    if (q < Lat<Q>::opp(q)) {
+      const float u = d[q], v = d[Lat<Q>::opp(q)];
+      d[q] = wall ? v : u;
+      d[Lat<Q>::opp(q)] = wall ? u : v;
+    }
   }
   if constexpr (FACES) {
-    if (!wall) {
-      const Geo& g = a.g;
+    const Geo& g = a.g;
+    uint32_t on = 0;
+#pragma unroll
+    for (int fi = 0; fi < 2; ++fi) {
+      const FaceK& fc = a.face[fi];
+      const uint32_t coord = fc.axis == 0 ? x.i0 : (fc.axis == 1 ? x.i1 : x.k);
+      const uint32_t nax = fc.axis == 0 ? g.n0 : (fc.axis == 1 ? g.n1 : g.n2);
+      if (fc.kind != kFaceNone && coord == (fc.side == 0 ? 0u : nax - 1)) on |= 1u << fi;
+    }
+    if (wall) on = 0;
+    if (__any_sync(__activemask(), on != 0)) {
 #pragma unroll
       for (int fi = 0; fi < 2; ++fi) {
+        if (!((on >> fi) & 1u)) continue;
         const FaceK& fc = a.face[fi];
-        if (fc.kind == kFaceNone) continue;
-        const uint32_t coord = fc.axis == 0 ? x.i0 : (fc.axis == 1 ? x.i1 : x.k);
-        const uint32_t nax = fc.axis == 0 ? g.n0 : (fc.axis == 1 ? g.n1 : g.n2);
-        if (coord != (fc.side == 0 ? 0u : nax - 1)) continue;
         if (fc.kind == kFacePressure) face_pressure<Q, float>(d, a, fi);
         else if (fc.kind == kFaceVelocity) face_velocity<Q, float>(d, a, fi);
         else face_zero_gradient_ref<Q, S, FORCE>(d, a, fi, x);
       }
     }
   }
+}
+
+// A wall byte, loaded where the source places it: the output warps fetch the
+// next plane's byte one plane ahead, and a volatile load is neither moved
+// towards its use nor repeated there by the compiler.
+__device__ __forceinline__ uint8_t ld_wall(const uint8_t* p) {
+  uint16_t v;
+  asm volatile("ld.global.nc.u8 %0, [%1];" : "=h"(v) : "l"(p));
+  return static_cast<uint8_t>(v);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -356,19 +381,20 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
 
   if (warp == 0) {
     // ---- producer: copy plane P into slot P % S once plane P - S is consumed
-    if (lane == 0) {
+    {
       PlaneRef L;
       plane_first<Q>(a, t, blockIdx.x, L);
       uint32_t P = 0;
       for (; L.item < t.items; plane_next<Q>(a, t, L), ++P) {
         const uint32_t sl = P % S_;
-        if (P >= S_ &&
-            !tile_wait(&sync->consumed[sl], (P / S_ - 1) & 1u, t.wait_ns, abort, 1024))
-          break;
+        const bool ok = P < S_ ||
+                        tile_wait(&sync->consumed[sl], (P / S_ - 1) & 1u, t.wait_ns, abort, 1024);
+        if (!__all_sync(0xffffffffu, ok)) break;
         fence_proxy_async_smem();
-        tiled_issue<Q>(a, t, L, planes + static_cast<size_t>(sl) * T::PLANE, &sync->full[sl]);
+        tiled_issue<Q>(a, t, L, planes + static_cast<size_t>(sl) * T::PLANE, &sync->full[sl],
+                       lane);
       }
-      sync->issued = P;
+      if (lane == 0) sync->issued = P;
     }
   } else if (warp <= static_cast<uint32_t>(T::NCW)) {
     // ---- collide warps: plane P in place once it has landed; lane cells
@@ -458,15 +484,14 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
       x.row = x.c - x.k;
       x.srow = x.row;
       if constexpr (MODE == kOutAoS) {
-        if (lane == 0) bulk_wait_read_all();  // the warp's previous store has read them
-        __syncwarp();
+        __syncwarp();  // the warp's previous copy has read the staging rows
       }
       uint8_t wb = 0;
       if (act && a.wall != nullptr) {
-        wb = x.c == wnext_c ? wnext : __ldg(a.wall + x.c);
+        wb = x.c == wnext_c ? wnext : ld_wall(a.wall + x.c);
         if (O.j < O.nv) {  // the same lane's cell of the next plane of this item
           wnext_c = x.c + t.SS;
-          wnext = __ldg(a.wall + wnext_c);
+          wnext = ld_wall(a.wall + wnext_c);
         }
       }
       R d[Q];
@@ -497,15 +522,19 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
         }
       }
       if constexpr (MODE == kOutAoS) {
-        // The warp's cells are a prefix of one contiguous run of the output.
-        // The proxy fence comes before this warp's global stores of the
-        // moments, so that it waits only for the staging writes.
+        // The warp's cells are a prefix of one contiguous run of the output
+        // that starts at a cell index divisible by 4 (tiles start at multiples
+        // of 32 along a2, rows hold a multiple of 4 cells) and holds a multiple
+        // of 4 cells: whole 16-byte groups, Q of them per 4 cells.
         const uint32_t nvalid = __popc(__ballot_sync(0xffffffffu, act));
-        fence_proxy_async_smem();
         __syncwarp();
-        if (lane == 0 && nvalid > 0)
-          bulk_store_s2g(static_cast<float*>(a.f_out) + static_cast<size_t>(x.c) * Q, wst,
-                         nvalid * Q * 4);
+        const float4* src = reinterpret_cast<const float4*>(wst);
+        float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.f_out) +
+                                                static_cast<size_t>(x.c - lane) * Q);
+        const uint32_t n4 = nvalid * Q / 4;
+#pragma unroll
+        for (uint32_t i = lane; i < 32 * Q / 4; i += 32)
+          if (i < n4) dst[i] = src[i];
       }
       if (act) {
         store_moments<Q, float>(a, x.c, mo, wall);
@@ -533,9 +562,7 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
         }
       }
     }
-    if constexpr (MODE == kOutAoS) {
-      if (lane == 0) bulk_wait_all();
-    }
+
   }
 
   __syncthreads();

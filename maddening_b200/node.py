@@ -25,9 +25,10 @@ Additions beyond the reference (documented extensions):
   contiguous extent is even, else one), ``1`` or ``2`` (also for FP32).  Every
   form gives bit-identical results.
 * ``one_pass`` -- ``update`` (and the first step of ``run``) reads the
-  reference-layout ``f`` once in a tiled kernel (default ``True``; FP32, FP16
-  and BF16 storage, last extent a multiple of 4) or runs as two passes
-  (``False``); the results are bit-identical.
+  reference-layout ``f`` once in a tiled kernel (last extent a multiple of 4)
+  or runs as two passes; the results are bit-identical.  ``None`` (default):
+  one pass, except that ``update`` with FP16/BF16 storage runs as two passes
+  (faster there); ``True``: one pass for every storage; ``False``: two passes.
 """
 
 from __future__ import annotations
@@ -97,7 +98,7 @@ class LBMNode(SimulationNode):
                  outlet_face: str = "x_max", geometry_source: Optional[str] = None,
                  *, outlet_condition: str = "pressure", storage: str = "f32",
                  device=None, cells_per_thread: Optional[int] = None,
-                 one_pass: bool = True):
+                 one_pass: Optional[bool] = None):
         lat = by_name(lattice)
         if len(grid_shape) != lat.D:
             raise ValueError(f"grid_shape has {len(grid_shape)} dims but lattice "
@@ -150,8 +151,10 @@ class LBMNode(SimulationNode):
             flags |= _lib.PLAN_SINGLE_CELLS
         elif cells_per_thread == 2:
             flags |= _lib.PLAN_PAIRED_CELLS
-        if not one_pass:
+        if one_pass is False:
             flags |= _lib.PLAN_TWO_PASS
+        elif one_pass:
+            flags |= _lib.PLAN_ONE_PASS_16BIT
         self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage, flags)
 
     # -- properties (lbm.py:690-703) ---------------------------------------
