@@ -156,6 +156,7 @@ class Plan:
         self.shape = tuple(int(n) for n in shape)
         self.tau = float(tau)
         self.storage = storage
+        self.flags = int(flags)
 
     @property
     def handle(self):

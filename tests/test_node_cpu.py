@@ -99,3 +99,17 @@ def test_no_cpu_path():
     node = LBMNode(name="lbm", timestep=0.001, grid_shape=(8, 8, 8))
     with pytest.raises(RuntimeError, match="CUDA"):
         node.initial_state()
+
+
+def test_one_pass_choice_sets_plan_flags():
+    """``one_pass=None`` leaves the choice to the library (one pass for FP32
+    storage, two passes for a single 16-bit update); True / False force it."""
+    from maddening_b200 import LBMNode, _lib
+    both = _lib.PLAN_TWO_PASS | _lib.PLAN_ONE_PASS_16BIT
+    for storage in ("f32", "f16", "bf16"):
+        node = LBMNode("n", 1.0, grid_shape=(8, 8, 8), storage=storage)
+        assert node.plan.flags & both == 0
+    assert LBMNode("n", 1.0, grid_shape=(8, 8, 8), storage="f16",
+                   one_pass=True).plan.flags & both == _lib.PLAN_ONE_PASS_16BIT
+    assert LBMNode("n", 1.0, grid_shape=(8, 8, 8),
+                   one_pass=False).plan.flags & both == _lib.PLAN_TWO_PASS
