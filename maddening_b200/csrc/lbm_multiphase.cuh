@@ -227,6 +227,13 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   if (c >= g.ncell) return;
   const Cell x = locate(g, c);
   const MPNbr o = mp_nbr(g, x);
+  // psi of the cell and of its 18 neighbours, loaded ahead of the wall test so
+  // that they travel with the population loads (only fluid cells use them)
+  const R* psi = static_cast<const R*>(a.psi);
+  R pn[19];
+  pn[0] = __ldg(psi + c);
+#pragma unroll
+  for (int q = 1; q < 19; ++q) pn[q] = __ldg(psi + mp_at(o, c, q, 1));
   const uint8_t* wm = a.s.wall;
   const bool wall = wm != nullptr && wm[c] != 0;
   R rho;
@@ -250,18 +257,17 @@ __global__ void __launch_bounds__(kBlock) k_mp_collide(const MPArgs a) {
   pipe_force<R>(a.s, c, wall, F);
   if (!wall) {
     // sum_q w_q psi(x + e_q) e_q = (2 S_axis + S_diag) / 36
-    const R* psi = static_cast<const R*>(a.psi);
     R s1[3] = {0, 0, 0}, s2[3] = {0, 0, 0};
 #pragma unroll
     for (int q = 1; q < 19; ++q) {
       const int e0 = Lat<19>::c0(q), e1 = Lat<19>::c1(q), e2 = Lat<19>::c2(q);
-      const R p = __ldg(psi + mp_at(o, c, q, 1));
+      const R p = pn[q];
       R(&acc)[3] = q <= 6 ? s1 : s2;
       if (e0) acc[0] = e0 > 0 ? add_r(acc[0], p) : sub_r(acc[0], p);
       if (e1) acc[1] = e1 > 0 ? add_r(acc[1], p) : sub_r(acc[1], p);
       if (e2) acc[2] = e2 > 0 ? add_r(acc[2], p) : sub_r(acc[2], p);
     }
-    const R coef = mul_r(static_cast<R>(-a.G), __ldg(psi + c));
+    const R coef = mul_r(static_cast<R>(-a.G), pn[0]);
     const R inv36 = static_cast<R>(1.0 / 36.0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) F[d] = fma_r(coef, mul_r(fma_r(R(2), s1[d], s2[d]), inv36), F[d]);
