@@ -584,7 +584,7 @@ def pipe_cost(dev, steps=200, grid=(384, 192, 192)):
     multiphase (G = -4.5, liquid 1.3 / gas 0.3, half filled).  Bytes per cell
     and step of the passes as built: single phase 152 (D3Q19) + 56 (D3Q7
     tracer) = 208 in one fused pass; multiphase 76 + 4 (density pass) + 76 + 4
-    + 76 (collide and push) = 236."""
+    + 76 (collide: pull, psi of the neighbours, aligned store) = 236."""
     import torch
     from maddening_b200.pipe import LBMPipeNode
     nx, ny, nz = grid
