@@ -705,10 +705,11 @@ def c1_cost(dev, grid=(64, 64, 64), steps=500):
     return out
 
 
-def update_call_cost(dev, grid=(256, 256, 256), calls=20):
+def update_call_cost(dev, grid=(256, 256, 256), calls=40):
     """One ``LBMNode.update`` call per step, as a graph manager drives the node
     (the reference-layout state in and out of every call), on the benchmark
-    workload; mean over ``calls`` calls.  The default one-pass tiled kernel
+    workload; mean over ``calls`` calls issued from Python, and over the same
+    calls captured once in a CUDA graph and replayed (``graph_ms_per_call``).  The default one-pass tiled kernel
     moves 173 B per cell (f in 76, wall 1, f out 76, density + velocity +
     pressure 20); the two-pass form (collide into the workspace, then the pull
     step) moves 324 and is timed beside it."""
@@ -729,21 +730,49 @@ def update_call_cost(dev, grid=(256, 256, 256), calls=20):
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(calls):
-            st = node.update(st, bi, 1.0)
-        e1.record()
-        torch.cuda.synchronize()
+        with ClockSampler(dev) as clk:  # the one pass is SM-bound: its time follows the clock
+            e0.record()
+            for _ in range(calls):
+                st = node.update(st, bi, 1.0)
+            e1.record()
+            torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / calls
+        sm = clk.summary()
+        # the same calls replayed from a CUDA graph: the device time per call
+        # without the Python side of update (which can fall behind a fast call)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            node.update(st, bi, 1.0)
+        torch.cuda.current_stream().wait_stream(side)
+        g = torch.cuda.CUDAGraph()
+        s_in = st
+        with torch.cuda.graph(g):
+            for _ in range(calls):
+                s_in = node.update(s_in, bi, 1.0)
+        g.replay()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        g.replay()
+        g1.record()
+        torch.cuda.synchronize()
+        ms_graph = g0.elapsed_time(g1) / calls
+        del g, s_in
         bpc = 173 if one_pass else 324
         frac = round(cells * bpc / (ms * 1e-3) / 1e9 / _peaks()[0], 4)
         if one_pass:
             res.update({"value": round(cells / ms / 1e3, 1), "unit": "MLUPS",
                         "ms_per_call": round(ms, 4), "bytes_per_cell": bpc, "hbm_frac": frac,
-                        "kernel": "k_tiled<19,float,kOutAoS,faces,no force> (one pass)"})
+                        "kernel": "k_tiled<19,float,kOutAoS,faces,no force> (one pass)",
+                        "sm_mhz": sm.get("sm_mhz"), "clock_reasons": sm.get("reasons"),
+                        "graph_ms_per_call": round(ms_graph, 4),
+                        "graph_mlups": round(cells / ms_graph / 1e3, 1)})
         else:
             res["two_pass"] = {"value": round(cells / ms / 1e3, 1), "ms_per_call": round(ms, 4),
-                               "bytes_per_cell": bpc, "hbm_frac": frac}
+                               "bytes_per_cell": bpc, "hbm_frac": frac, "sm_mhz": sm.get("sm_mhz"),
+                               "graph_ms_per_call": round(ms_graph, 4)}
         del node, st
         torch.cuda.empty_cache()
     return res

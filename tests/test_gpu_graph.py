@@ -34,16 +34,16 @@ def test_captured_rollout_equals_plain(storage):
             assert torch.equal(out[key], ref[key]), key
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16"])
-def test_captured_update_calls_equal_plain(storage):
-    """Three chained ``update`` calls (the one-pass kernel: the call a graph
-    manager makes each step) captured once and replayed give the plain calls'
-    bytes."""
+@pytest.mark.parametrize("storage,one_pass", [("f32", None), ("f16", None), ("f16", True)])
+def test_captured_update_calls_equal_plain(storage, one_pass):
+    """Three chained ``update`` calls (the call a graph manager makes each
+    step: the one-pass kernel, or two passes for a default 16-bit plan)
+    captured once and replayed give the plain calls' bytes."""
     from maddening_b200 import LBMNode
     grid = (20, 16, 36)
     rng = np.random.default_rng(2)
     node = LBMNode("u", 1.0, grid_shape=grid, viscosity=0.05, wall_mask=rng.random(grid) < 0.1,
-                   outlet_condition="zero_gradient", storage=storage)
+                   outlet_condition="zero_gradient", storage=storage, one_pass=one_pass)
     bi = {"inlet_velocity": np.array([0.04, 0.0, 0.0], dtype=np.float32)}
     st = node.initial_state()
 
