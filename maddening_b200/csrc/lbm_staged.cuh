@@ -1,6 +1,7 @@
 // Asynchronous-copy helpers of the one-pass tiled step (lbm_tiled.cuh): 1-D
-// bulk copies from global into this CTA's shared memory (cp.async.bulk) with
-// their completion tracked by an mbarrier.
+// bulk copies between global and this CTA's shared memory (cp.async.bulk),
+// completion tracked by an mbarrier for loads and by the issuing thread's
+// bulk async-group for stores.
 #pragma once
 
 #include "lbm_kernels.cuh"
@@ -52,6 +53,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
   return ok != 0;
+}
+
+// This CTA's shared memory -> global, `bytes` a multiple of 16, both addresses
+// 16-byte aligned; tracked in the issuing thread's bulk async-group, which
+// this call commits.
+__device__ __forceinline__ void bulk_store_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// All but the issuing thread's most recent bulk store have finished reading
+// shared memory.
+__device__ __forceinline__ void bulk_wait_read_1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+
+// The issuing thread's bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 }  // namespace lbm

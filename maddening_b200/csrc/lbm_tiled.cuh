@@ -23,9 +23,9 @@
 //     output warps, one per 32-cell tile row, pull the collided populations of
 //     plane P from slots P - 1, P, P + 1 once P + 1 is collided, apply the
 //     wall swap and the faces, take the moments and write f_bc (kOutAoS:
-//     staged per warp in shared memory, then written as whole 16-byte groups
-//     of the warp's contiguous run) or collide again and write the next state
-//     planes (kOutState: the first step of a rollout).  Collide warps run up
+//     staged per warp in shared memory, two staging rows used in turn, and
+//     written by a bulk asynchronous store) or collide again and write the
+//     next state planes (kOutState: the first step of a rollout).  Collide warps run up
 //     to a few planes ahead of the output warps.
 //   * A persistent grid walks work items (column, chunk of planes along the
 //     sweep); blocks take items with a grid stride in chunk-major order, so
@@ -106,7 +106,7 @@ struct TileSync {
 
 template <int Q, int MODE>
 __host__ __device__ constexpr size_t tiled_stage_bytes() {
-  return MODE == kOutAoS ? static_cast<size_t>(TileShape<Q>::NOW) * 32 * Q * 4 : 0;
+  return MODE == kOutAoS ? static_cast<size_t>(TileShape<Q>::NOW) * 2 * 32 * Q * 4 : 0;
 }
 template <int Q, int MODE>
 __host__ __device__ constexpr size_t tiled_smem_bytes() {
@@ -456,7 +456,10 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
     // ---- output warps: tile row `ty` of plane P once P + 1 is collided
     const uint32_t ow = warp - 1 - T::NCW;
     const uint32_t ty = ow / (T::TZ / 32), tz = (ow % (T::TZ / 32)) * 32 + lane;
-    float* wst = stage + static_cast<size_t>(ow) * 32 * Q;  // this warp's staging rows
+    // this warp's two staging rows, used in turn: a plane's store may still be
+    // reading one while the next plane is staged in the other
+    float* const wst2 = stage + static_cast<size_t>(ow) * 2 * 32 * Q;
+    uint32_t nstore = 0;  // bulk stores this warp has issued
     const uint32_t off = ((ty + T::HR) * T::W + kTileHalo + tz) * Q;  // own cell in a slot
     PlaneRef O;
     plane_first<Q>(a, t, blockIdx.x, O);
@@ -483,8 +486,11 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
       x.c = ps * t.SS + (O.y0 + ty) * t.SR + x.k;
       x.row = x.c - x.k;
       x.srow = x.row;
+      float* const wst = wst2 + (nstore & 1u) * 32 * Q;
       if constexpr (MODE == kOutAoS) {
-        __syncwarp();  // the warp's previous copy has read the staging rows
+        // the store before the last one has finished reading this staging row
+        if (lane == 0) bulk_wait_read_1();
+        __syncwarp();
       }
       uint8_t wb = 0;
       if (act && a.wall != nullptr) {
@@ -522,19 +528,16 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
         }
       }
       if constexpr (MODE == kOutAoS) {
-        // The warp's cells are a prefix of one contiguous run of the output
-        // that starts at a cell index divisible by 4 (tiles start at multiples
-        // of 32 along a2, rows hold a multiple of 4 cells) and holds a multiple
-        // of 4 cells: whole 16-byte groups, Q of them per 4 cells.
+        // The warp's cells are a prefix of one contiguous run of the output.
+        // The proxy fence comes before this warp's global stores of the
+        // moments, so that it waits only for the staging writes.
         const uint32_t nvalid = __popc(__ballot_sync(0xffffffffu, act));
+        fence_proxy_async_smem();
         __syncwarp();
-        const float4* src = reinterpret_cast<const float4*>(wst);
-        float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.f_out) +
-                                                static_cast<size_t>(x.c - lane) * Q);
-        const uint32_t n4 = nvalid * Q / 4;
-#pragma unroll
-        for (uint32_t i = lane; i < 32 * Q / 4; i += 32)
-          if (i < n4) dst[i] = src[i];
+        if (lane == 0 && nvalid > 0)
+          bulk_store_s2g(static_cast<float*>(a.f_out) + static_cast<size_t>(x.c) * Q, wst,
+                         nvalid * Q * 4);
+        nstore += nvalid > 0 ? 1u : 0u;
       }
       if (act) {
         store_moments<Q, float>(a, x.c, mo, wall);
@@ -562,7 +565,9 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
         }
       }
     }
-
+    if constexpr (MODE == kOutAoS) {
+      if (lane == 0) bulk_wait_all();
+    }
   }
 
   __syncthreads();
