@@ -420,6 +420,8 @@ def run_ours(args):
         torch.cuda.empty_cache()
         variants["frames"] = frames_cost(dev)
         torch.cuda.empty_cache()
+        variants["sharded"] = sharded_cost(dev)
+        torch.cuda.empty_cache()
         variants["precision_512"] = precision_cost(dev, args.c5_steps)
 
     upd = update_call_cost(dev) if (rank == 0 and not args.no_variants) else None
@@ -778,6 +780,52 @@ def update_call_cost(dev, grid=(256, 256, 256), calls=40):
     return res
 
 
+def sharded_cost(dev, grid=(256, 256, 256), steps=20):
+    """The slab-sharded runner (``ShardedLBM``) with one rank on this GPU: the
+    256^3 lattice with the benchmark's spheres and a body force along x (no
+    faces: the sharded axis 0 carries none), FP32; per step one state step of
+    the padded slab and the pad refresh of the 5 crossing populations of each
+    face, issued from Python.  Timed beside ``LBMNode.run`` of the same lattice
+    (CUDA events, best of three)."""
+    import torch
+    from maddening_b200 import LBMNode
+    from maddening_b200.geometry import random_spheres
+    from maddening_b200.sharded import ShardedLBM
+    cells = grid[0] * grid[1] * grid[2]
+    node = LBMNode("sharded", 1.0, grid_shape=grid, viscosity=(TAU - 0.5) / 3.0,
+                   wall_mask=random_spheres(grid, seed=0), device=dev)
+    bi = {"body_force": np.array([1e-6, 0.0, 0.0], dtype=np.float32)}
+    st = node.initial_state()
+    sh = ShardedLBM(node)
+    sh.scatter(st)
+    sh.run(bi, 3)
+
+    def best(fn):
+        t = float("inf")
+        for _ in range(3):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t = min(t, e0.elapsed_time(e1))
+        return t
+
+    t_sh = best(lambda: sh.run(bi, steps))
+    node.run(st, bi, 3)
+    t_run = best(lambda: node.run(st, bi, steps))
+    del sh
+    return {"workload": "%s spheres + body force, FP32, %d steps, one rank"
+                        % ("x".join(map(str, grid)), steps),
+            "sharded_mlups": round(cells * steps / t_sh / 1e3, 1),
+            "run_mlups": round(cells * steps / t_run / 1e3, 1),
+            "sharded_over_run": round(t_run / t_sh, 3),
+            "note": "node.run includes its first collide from the reference layout and the "
+                    "last step back to it; the sharded steps stay in the state layout"}
+
+
 def frames_cost(dev, grid=(256, 256, 256), frames=20):
     """Streaming frames of a running node (BinaryStateEncoder over density and
     velocity of the benchmark lattice, 16 B per cell): the one-launch device
@@ -905,7 +953,8 @@ def main():
                     help="cube side (256 = the benchmark workload; smaller for profiling)")
     ap.add_argument("--c5-steps", type=int, default=2000,
                     help="steps of the 512^3 precision comparison (variants)")
-    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9", "c1", "batched"],
+    ap.add_argument("--only", choices=["pipe", "update_call", "frames", "d2q9", "c1", "batched",
+                                       "sharded"],
                     help="run one variant alone and print its JSON (for profiling)")
     ap.add_argument("--variant-grid", default=None,
                     help="lattice of --only, e.g. 192x128x128 (default: the variant's own)")
@@ -921,7 +970,8 @@ def main():
         if args.variant_grid and args.only != "batched":
             kw["grid"] = tuple(int(v) for v in args.variant_grid.split("x"))
         fn = {"pipe": pipe_cost, "update_call": update_call_cost, "frames": frames_cost,
-              "d2q9": d2q9_cost, "c1": c1_cost, "batched": batched_cost}[args.only]
+              "d2q9": d2q9_cost, "c1": c1_cost, "batched": batched_cost,
+              "sharded": sharded_cost}[args.only]
         if args.only == "pipe":
             kw["steps"] = args.steps
         print(json.dumps({args.only: fn(dev, **kw)}), flush=True)

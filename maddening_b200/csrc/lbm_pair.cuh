@@ -437,21 +437,26 @@ __device__ __forceinline__ void gpair_step(const StepArgs& a, uint32_t pidx) {
   const uint32_t dp1 = i1 == g.n1 - 1 ? 0u - (g.n1 - 1) * g.rstride : g.rstride;
   const uint32_t kprev = (k == 0 ? g.rstride : k) - 2u;
   const uint32_t knext = k + 2 == g.rstride ? 0u : k + 2;
-  const S* pin = static_cast<const S*>(a.pin);
+  // addresses relative to this pair in plane 0: q pstride plus the row
+  // deltas is never negative (q = 0 has none; q >= 1 adds at least one plane
+  // of pstride >= splane + rstride), so it extends as unsigned
+  const S* b0 = static_cast<const S*>(a.pin) + (srow + k);
+  const int32_t ep = static_cast<int32_t>(kprev) - static_cast<int32_t>(k);
+  const int32_t en = static_cast<int32_t>(knext) - static_cast<int32_t>(k);
   P v[Q];
   P e[Q];
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const int c0 = Lat<Q>::c0(q), c1 = Lat<Q>::c1(q), c2 = Lat<Q>::c2(q);
-    uint32_t off = srow;
+    uint32_t off = static_cast<uint32_t>(q) * g.pstride;
     if (c0 > 0) off += dm0;
     if (c0 < 0) off += dp0;
     if (c1 > 0) off += dm1;
     if (c1 < 0) off += dp1;
-    const S* base = pin + (static_cast<uint32_t>(q) * g.pstride + off);
-    v[q] = PT::ld(base + k);
-    if (c2 > 0) e[q] = PT::ld(base + kprev);
-    if (c2 < 0) e[q] = PT::ld(base + knext);
+    const S* base = b0 + off;
+    v[q] = PT::ld(base);
+    if (c2 > 0) e[q] = PT::ld(base + ep);
+    if (c2 < 0) e[q] = PT::ld(base + en);
   }
   pair_finish<Q, S, FACES, FORCE, PAD>(a, i0, i1, k, r * g.n2, srow, v, e, valid);
 }
