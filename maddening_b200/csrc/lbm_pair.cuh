@@ -262,8 +262,13 @@ struct QuadT {
 #ifndef LBM_QUAD19_MIN_WARPS
 #define LBM_QUAD19_MIN_WARPS 20
 #endif
+// D2Q9 four-cell budget (B200 sweep, 4096^2 channel FP16: 24 / 32 / 40 / 48
+// resident warps 134.9k / 138.5k / 125.0k / 98.9k MLUPS).
+#ifndef LBM_QUAD9_MIN_WARPS
+#define LBM_QUAD9_MIN_WARPS LBM_PAIR_MIN_WARPS
+#endif
 template <int Q>
-constexpr int quad_min_warps() { return Q == 19 ? LBM_QUAD19_MIN_WARPS : kPairMinWarps; }
+constexpr int quad_min_warps() { return Q == 19 ? LBM_QUAD19_MIN_WARPS : LBM_QUAD9_MIN_WARPS; }
 
 // The populations of quad (k..k+3) of source row `base` pulled along the row:
 // kprev / knext the aligned 32-bit words holding cells k - 1 / k + 4
