@@ -4,7 +4,7 @@
   (float32 state between steps, like the reference's float32 path) and
   fused ``run`` (offsets kept on the device), FP32 and FP64 storage;
 * the 64^3 force-driven channel, 500 steps, FP32 vs the FP64 oracle: relative
-  L2 of density and velocity <= 1e-5 (the north-star bound);
+  L2 of density and velocity <= 1e-5 (the FP32 accuracy bound);
 * the benchmark's obstacle flow (seeded spheres, velocity inlet 0.05,
   zero-gradient outlet) at 64^3, 500 steps: FP32 <= 1e-5 and FP16 storage
   <= 1e-3 against the FP64 oracle's run (tests/golden/obstacle64.npz);
