@@ -223,7 +223,7 @@ def host_info():
     except OSError:
         pass
     return {"cpu_model": model, "cpu_count": os.cpu_count(), "affinity": _host_cores(),
-            "reference_runtime": "reference JAX CPU path unavailable on this box (jax is not "
+            "reference_runtime": "reference JAX CPU path unavailable on this machine (jax is not "
                                  "installed and has no offline wheel); the float32 "
                                  "restatement of the reference step stands in"}
 
