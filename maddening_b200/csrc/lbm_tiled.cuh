@@ -54,11 +54,14 @@ template <int Q>
 struct Sweep;
 template <>
 struct Sweep<19> {
-  static constexpr int TY = 8, TZ = 32;  // tile rows (a1) x row cells (a2)
-  static constexpr int HR = 1;           // halo rows
-  static constexpr int NCW = 7;          // collide warps, two cells per lane over the
-  static constexpr int CPL = 2;          //   (8 + 2) x 40 buffered cells <= 7 x 32 x 2
-  static constexpr int MINB = 1;         // resident blocks per SM
+  static constexpr int TY = 10, TZ = 32;  // tile rows (a1) x row cells (a2)
+  static constexpr int HR = 1;            // halo rows
+  static constexpr int NCW = 8;           // collide warps, two cells per lane over the
+  static constexpr int CPL = 2;           //   (10 + 2) x 40 buffered cells <= 8 x 32 x 2
+  static constexpr int MINB = 1;          // resident blocks per SM
+  // plane slots: 3 read by the output warps, one being collided, one landing
+  // (the ring and two staging rows per output warp fill 226 KB of shared memory)
+  static constexpr int SLOTS = 5;
   __host__ __device__ static constexpr int cs(int q) { return Lat<19>::c0(q); }  // sweep
   __host__ __device__ static constexpr int cr(int q) { return Lat<19>::c1(q); }  // rows
 };
@@ -69,12 +72,13 @@ struct Sweep<9> {
   static constexpr int NCW = 3;  // 136 buffered cells <= 3 x 32 x 2
   static constexpr int CPL = 2;
   static constexpr int MINB = 2;
+  static constexpr int SLOTS = 6;  // two planes landing ahead of the collide
   __host__ __device__ static constexpr int cs(int q) { return Lat<9>::c1(q); }
   __host__ __device__ static constexpr int cr(int) { return 0; }
 };
 
 constexpr int kTileHalo = 4;   // cells copied on each side of a tile row
-constexpr int kTileSlots = 6;  // plane slots: 3 read by the output warps, the rest ahead
+constexpr int kMaxTileSlots = 6;  // plane slots of the deepest ring (Sweep<Q>::SLOTS)
 
 template <int Q>
 struct TileShape {
@@ -96,9 +100,9 @@ struct TileShape {
 
 // Barriers and flags of a block, after the slots and the staging rows.
 struct TileSync {
-  uint64_t full[kTileSlots];      // plane landed (producer arrive + copy bytes)
-  uint64_t collided[kTileSlots];  // plane collided (one arrive per collide warp)
-  uint64_t consumed[kTileSlots];  // plane read for the last time (one per output warp)
+  uint64_t full[kMaxTileSlots];      // plane landed (producer arrive + copy bytes)
+  uint64_t collided[kMaxTileSlots];  // plane collided (one arrive per collide warp)
+  uint64_t consumed[kMaxTileSlots];  // plane read for the last time (one per output warp)
   int abort;                      // a wait gave up
   uint32_t issued;                // planes copied by the producer
   uint32_t landed;                // planes a collide warp has seen land
@@ -110,7 +114,7 @@ __host__ __device__ constexpr size_t tiled_stage_bytes() {
 }
 template <int Q, int MODE>
 __host__ __device__ constexpr size_t tiled_smem_bytes() {
-  return static_cast<size_t>(kTileSlots) * TileShape<Q>::PLANE * 4 + tiled_stage_bytes<Q, MODE>() +
+  return static_cast<size_t>(Sweep<Q>::SLOTS) * TileShape<Q>::PLANE * 4 + tiled_stage_bytes<Q, MODE>() +
          sizeof(TileSync);
 }
 
@@ -355,7 +359,8 @@ __global__ void __launch_bounds__(TileShape<Q>::NT, Sweep<Q>::MINB)
   using T = TileShape<Q>;
   using R = float;
   static_assert(MODE == kOutAoS || MODE == kOutState, "f_bc out or the next state out");
-  constexpr uint32_t S_ = kTileSlots;
+  constexpr uint32_t S_ = Sweep<Q>::SLOTS;
+  static_assert(Sweep<Q>::SLOTS >= 5 && Sweep<Q>::SLOTS <= kMaxTileSlots, "ring depth");
   extern __shared__ __align__(128) unsigned char smem[];
   float* planes = reinterpret_cast<float*>(smem);
   float* stage = planes + static_cast<size_t>(S_) * T::PLANE;
