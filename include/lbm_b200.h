@@ -82,7 +82,8 @@ typedef struct {
 
 /* lbm_desc.flags */
 /* bit 1u is reserved (an earlier row-staged rollout step, slower than the
-   default gather, was removed) and rejected by lbm_plan_create */
+   default gather, was removed) and rejected by lbm_plan_create; so is every
+   bit not defined below */
 #define LBM_PLAN_SINGLE_CELLS 2u /* rollout steps update one cell per thread
                                    (FP16/BF16 storage otherwise takes the
                                    four-cell step on rows of a multiple of 256
@@ -101,16 +102,6 @@ typedef struct {
                                 run out: it sets the status word and returns
                                 early with the outputs incomplete.  Only for
                                 testing the timeout path */
-#define LBM_PLAN_ONE_PASS_16BIT 32u /* lbm_update with FP16/BF16 storage also runs
-                                the one-pass tiled kernel.  By default a single
-                                update with 16-bit storage runs as two passes,
-                                which move 248 B per D3Q19 cell and measure
-                                faster there than the one pass (whose collides
-                                round every halo cell stochastically); FP32
-                                storage takes the one pass by default.  The
-                                first step of lbm_rollout takes the one pass
-                                for every 32-bit-IO storage unless
-                                LBM_PLAN_TWO_PASS is set */
 
 typedef struct {
   int32_t lattice;  /* lbm_lattice: 19 (D3Q19) or 9 (D2Q9)                */

@@ -39,7 +39,6 @@ PLAN_SINGLE_CELLS = 2
 PLAN_PAIRED_CELLS = 4
 PLAN_TWO_PASS = 8
 PLAN_TEST_WAIT_TIMEOUT = 16
-PLAN_ONE_PASS_16BIT = 32
 
 
 class lbm_desc(C.Structure):

@@ -391,9 +391,7 @@ int run_steps(const lbm_plan* p, cudaStream_t s, lbm::StepArgs a, const void* f_
   a.f_out = f_out;
   int rc;
   if constexpr (sizeof(typename lbm::StoreT<S>::IO) == 4) {
-    // a single update: one pass for FP32 storage, for 16-bit storage on request
-    const bool one = sizeof(S) == 4 || (p->flags & LBM_PLAN_ONE_PASS_16BIT);
-    if (n == 1 && one && tiled_ok<S>(p, a, ws, true)) {
+    if (n == 1 && tiled_ok<S>(p, a, ws, true)) {
       // the whole update in one pass; the workspace holds only the status word
       a.status = reinterpret_cast<int*>(ws);
       rc = cuda_check(cudaMemsetAsync(a.status, 0, sizeof(int), s), "cudaMemsetAsync");
@@ -879,8 +877,7 @@ int lbm_plan_create(const lbm_desc* desc, lbm_plan** plan) {
   if (!(desc->tau > 0.5) || !std::isfinite(desc->tau))
     return fail(LBM_ERR_INVALID, "tau must be > 0.5 (got %g). Increase viscosity.", desc->tau);
   constexpr uint32_t kKnownFlags = LBM_PLAN_SINGLE_CELLS | LBM_PLAN_PAIRED_CELLS |
-                                   LBM_PLAN_TWO_PASS | LBM_PLAN_TEST_WAIT_TIMEOUT |
-                                   LBM_PLAN_ONE_PASS_16BIT;
+                                   LBM_PLAN_TWO_PASS | LBM_PLAN_TEST_WAIT_TIMEOUT;
   if (desc->flags & ~kKnownFlags)
     return fail(LBM_ERR_INVALID, "unknown or reserved plan flags 0x%x",
                 static_cast<unsigned>(desc->flags & ~kKnownFlags));

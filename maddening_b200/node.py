@@ -25,10 +25,9 @@ Additions beyond the reference (documented extensions):
   contiguous extent is even, else one), ``1`` or ``2`` (also for FP32).  Every
   form gives bit-identical results.
 * ``one_pass`` -- ``update`` (and the first step of ``run``) reads the
-  reference-layout ``f`` once in a tiled kernel (last extent a multiple of 4)
-  or runs as two passes; the results are bit-identical.  ``None`` (default):
-  one pass, except that ``update`` with FP16/BF16 storage runs as two passes
-  (faster there); ``True``: one pass for every storage; ``False``: two passes.
+  reference-layout ``f`` once in a tiled kernel (``None`` or ``True``, the
+  default; FP32, FP16 and BF16 storage, last extent a multiple of 4) or runs
+  as two passes (``False``); the results are bit-identical.
 """
 
 from __future__ import annotations
@@ -153,8 +152,6 @@ class LBMNode(SimulationNode):
             flags |= _lib.PLAN_PAIRED_CELLS
         if one_pass is False:
             flags |= _lib.PLAN_TWO_PASS
-        elif one_pass:
-            flags |= _lib.PLAN_ONE_PASS_16BIT
         self._plan = _lib.Plan(lat.Q, self._grid_shape, tau, storage, flags)
 
     # -- properties (lbm.py:690-703) ---------------------------------------

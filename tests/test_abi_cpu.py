@@ -126,8 +126,7 @@ def test_update_padded_rejects_blocks_without_a_halo_before_any_device_work():
 
 def test_plan_rejects_unknown_and_reserved_flags():
     from maddening_b200 import _lib
-    for flags in (1, 64, 1 << 30):
+    for flags in (1, 32, 64, 1 << 30):
         with pytest.raises(_lib.LbmError, match="reserved plan flags"):
             _lib.Plan(19, (8, 8, 8), 0.8, "f32", flags=flags)
     _lib.Plan(19, (8, 8, 8), 0.8, "f32", flags=_lib.PLAN_TWO_PASS | _lib.PLAN_SINGLE_CELLS)
-    _lib.Plan(19, (8, 8, 8), 0.8, "f16", flags=_lib.PLAN_ONE_PASS_16BIT)

@@ -102,14 +102,11 @@ def test_no_cpu_path():
 
 
 def test_one_pass_choice_sets_plan_flags():
-    """``one_pass=None`` leaves the choice to the library (one pass for FP32
-    storage, two passes for a single 16-bit update); True / False force it."""
+    """``one_pass`` None / True keep the library's one pass; False asks for two."""
     from maddening_b200 import LBMNode, _lib
-    both = _lib.PLAN_TWO_PASS | _lib.PLAN_ONE_PASS_16BIT
     for storage in ("f32", "f16", "bf16"):
-        node = LBMNode("n", 1.0, grid_shape=(8, 8, 8), storage=storage)
-        assert node.plan.flags & both == 0
-    assert LBMNode("n", 1.0, grid_shape=(8, 8, 8), storage="f16",
-                   one_pass=True).plan.flags & both == _lib.PLAN_ONE_PASS_16BIT
-    assert LBMNode("n", 1.0, grid_shape=(8, 8, 8),
-                   one_pass=False).plan.flags & both == _lib.PLAN_TWO_PASS
+        for one in (None, True):
+            node = LBMNode("n", 1.0, grid_shape=(8, 8, 8), storage=storage, one_pass=one)
+            assert node.plan.flags & _lib.PLAN_TWO_PASS == 0
+        assert LBMNode("n", 1.0, grid_shape=(8, 8, 8), storage=storage,
+                       one_pass=False).plan.flags & _lib.PLAN_TWO_PASS
